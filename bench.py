@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 cut-rank DP executor on the n=70, width-30 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gsb|reference]
+
+Workload: n = 70 random graph-state circuit of depth 70 (CZ on seeded random perfect matchings + seeded random
+single-qubit Cliffords, seed 2), Haar-random U3 layer, order of width 30 from the native order search (seed 12):
+an arena of 2^30 entries (8.6 GB complex64, 17.2 GB complex128).  The arena is far larger than L2 (126 MB), so
+every pass streams from HBM and no flush is needed between steps.
+
+One step = the exact amplitudes (log2 Pr and all 70 conditionals, 'chain' mode: one pass per DP step) of
+--amps-per-step uniform random bitstrings in the complex64 form.  `value` is amplitudes/s with the strings already
+in HBM (device-resident entry point), timed with CUDA events on the engine's stream, max over ranks; `e2e` is the
+same metric through the host-buffer C-ABI call (strings copied in from pinned host memory, log2 Pr and
+conditionals copied back, every step).  Extra keys report exact samples (s/sample, two passes per DP step), the
+complex128 form, the complex64-vs-complex128 agreement, the roofline of the dominant kernel and the reference's CPU
+executor timed on this host.
+
+Multi-GPU: replicas only (the arena sweep does not shard without an all-to-all per step): each rank evaluates its
+own strings on its own GPU; value = all ranks' amplitudes / the slowest rank's time.
+
+--impl reference times the reference's own CPU executor (gsamp2 compiled from its sources into oracle/_ref, complex64,
+'chain' mode, every host core) on one string of the same workload per step, on rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "exact-graphstate-sampling_b200")
+sys.path.insert(0, PKG)
+sys.path.insert(0, ROOT)
+
+METRIC = "s/sample & amps/s at n=70 w=30, c64 form vs c128 plain, |Δlog2P|≤1e-5; HBM GB/s"
+WORKLOAD = "matching_n70_d70_s2_w30"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="gsb", choices=["gsb", "reference"])
+    ap.add_argument("--amps-per-step", type=int, default=16)
+    ap.add_argument("--samples", type=int, default=16)
+    ap.add_argument("--c128-amps", type=int, default=8)
+    ap.add_argument("--c128-samples", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples every 200 ms while running (SM clock, max clock, throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p:
+            self.p.terminate()
+            try:
+                self.p.wait(5)
+            except subprocess.TimeoutExpired:
+                self.p.kill()
+
+    def summary(self):
+        self.f.flush()
+        rows = []
+        for ln in open(self.f.name):
+            t = [x.strip() for x in ln.split(",")]
+            if len(t) >= 9:
+                try:
+                    rows.append((float(t[1]), float(t[2]), t[5:9]))
+                except ValueError:
+                    pass
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init(n):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return rank, world, local
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def ref_chain_time(plan_path, strings_path, threads):
+    """Wall time of the reference executor ('chain' mode, complex64) on the strings file, and its stdout."""
+    from oracle import ref_binary, run_ref
+    t0 = time.perf_counter()
+    if ref_binary(64):
+        out = run_ref(64, [plan_path, "chain", strings_path], threads=threads)
+        kind = "reference"
+    else:
+        from oracle import Oracle
+        o = Oracle(plan_path, 64)
+        out = ""
+        for ln in open(strings_path):
+            if ln.strip():
+                lp, _ = o.chain1(ln.strip())
+                out += f"{lp:.12f}\n"
+        kind = "port"
+    return time.perf_counter() - t0, out, kind
+
+
+def run_reference(args):
+    rank, world, local = dist_init(args.gpus)
+    if rank != 0:
+        return
+    import workloads
+    w = workloads.matching_n70_w30()
+    cores = os.cpu_count() or 1
+    strings = workloads.random_strings(len(w["steps"]), args.warmup + args.steps, seed=4242)
+    with tempfile.TemporaryDirectory() as td:
+        plan = os.path.join(td, "plan.txt")
+        open(plan, "w").write(w["plan"])
+        times = []
+        kind = "reference"
+        for i in range(args.warmup + args.steps):
+            sp = os.path.join(td, f"s{i}.txt")
+            open(sp, "w").write("".join(str(int(b)) for b in strings[i]) + "\n")
+            t, _, kind = ref_chain_time(plan, sp, cores)
+            if i >= args.warmup:
+                times.append(t)
+    tot = sum(times)
+    v = args.steps / tot
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "amps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "c64 arena, f64 arithmetic", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": 70, "width": w["width"], "strings_per_step": 1, "mode": "chain",
+                   "l2": "arena 8.6 GB >> L2"},
+        "cpu_baseline": {"value": v, "unit": "amps/s", "cores": cores, "kind": kind,
+                         "sample": f"{args.steps} uniform random strings of the workload, one per step, gsamp2 chain "
+                                   f"mode, OMP_NUM_THREADS={cores}"},
+        "e2e": {"value": v, "unit": "amps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+def run_gsb(args):
+    import numpy as np
+    import torch
+    rank, world, local = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    import gsb
+    import workloads
+    w = workloads.matching_n70_w30()
+    steps = w["steps"]
+    ns = len(steps)
+    A, K, W = args.amps_per_step, args.steps, args.warmup
+    hbm_peak, peak_kind = peaks()
+
+    eng = gsb.Engine.from_text(w["plan"], precision=64, device=local)
+    stream = torch.cuda.current_stream()
+    eng.set_stream(stream.cuda_stream)
+    strings = workloads.random_strings(ns, (W + K) * A, seed=1000 + rank)
+    d_bits = torch.from_numpy(strings).to("cuda")
+    d_lp = torch.empty((W + K) * A, dtype=torch.float64, device="cuda")
+    d_cond = torch.empty(((W + K) * A, ns), dtype=torch.float64, device="cuda")
+
+    def amp_step(i):
+        sl = slice(i * A, (i + 1) * A)
+        eng.chain_device(d_bits[sl], d_lp[sl], d_cond[sl])
+
+    for i in range(W):
+        amp_step(i)
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for i in range(W, W + K):
+            amp_step(i)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms, world)
+    value = world * K * A / (ms_max / 1000.0)
+    lp64 = d_lp.cpu().numpy()
+    cond64 = d_cond.cpu().numpy()
+
+    # e2e: host strings (pinned) -> C ABI -> host results, every step
+    pinned = torch.from_numpy(strings[W * A:(W + K) * A].copy()).pin_memory()
+    host = pinned.numpy()
+    eng.chain(host[:A])
+    torch.cuda.synchronize()
+    barrier(world)
+    t0 = time.perf_counter()
+    for i in range(K):
+        eng.chain(host[i * A:(i + 1) * A])
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e = {"value": world * K * A / e2e_s, "unit": "amps/s", "h2d_bytes_per_step": A * ns,
+           "d2h_bytes_per_step": A * 8 + A * ns * 8}
+
+    # exact samples (two passes per DP step), device-resident uniforms
+    S = args.samples
+    rng = np.random.default_rng(77 + rank)
+    d_u = torch.from_numpy(rng.random((S, ns))).to("cuda")
+    d_sb = torch.empty((S, ns), dtype=torch.int8, device="cuda")
+    d_slp = torch.empty(S, dtype=torch.float64, device="cuda")
+    eng.sample_device(d_u[:1], d_sb[:1], d_slp[:1])
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    eng.sample_device(d_u, d_sb, d_slp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    s_per_sample64 = max_over_ranks(e0.elapsed_time(e1) / 1000.0 / S, world)
+    sbits64 = d_sb.cpu().numpy()
+
+    # roofline of the dominant kernel (the write pass, k_step<float2,...,true>): per-step event timing
+    tot_bytes, per = workloads.pass_bytes(steps, 8, "chain")
+    wsum = np.zeros(ns)
+    nprof = 3
+    for j in range(nprof):
+        wm, _ = eng.profile_steps(strings[j])
+        wsum += wm
+    wmean = wsum / nprof
+    bytes_w = sum(p[0] for p in per)
+    achieved = bytes_w / (wmean.sum() / 1000.0) / 1e9
+    # per-step detail of the widest steps
+    wide = [k for k in range(ns) if steps[k]["r"] >= 27]
+    wide_bytes = sum(per[k][0] for k in wide)
+    wide_ms = float(wmean[wide].sum())
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "write_pass_traffic.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath)).get("dram_bytes_per_string_c64")
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
+                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_step<float2,*,*,*,write>",
+                "algorithmic_bytes_per_string": bytes_w, "kernel_ms_per_string": float(wmean.sum()),
+                "wide_steps_frac": (wide_bytes / (wide_ms / 1000.0) / 1e9) / hbm_peak if wide_ms > 0 else None}
+    eng.close()
+
+    # complex128 plain form on the first strings of the timed batch, and the c64-vs-c128 agreement
+    c128 = {}
+    if args.c128_amps > 0:
+        e128 = gsb.Engine.from_text(w["plan"], precision=128, device=local)
+        e128.set_stream(stream.cuda_stream)
+        B = args.c128_amps
+        d_lp128 = torch.empty(B, dtype=torch.float64, device="cuda")
+        d_cond128 = torch.empty((B, ns), dtype=torch.float64, device="cuda")
+        sl = slice(W * A, W * A + B)
+        e128.chain_device(d_bits[:1], d_lp128[:1], d_cond128[:1])
+        torch.cuda.synchronize()
+        e0.record(stream)
+        e128.chain_device(d_bits[sl], d_lp128, d_cond128)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        amps128 = B / (e0.elapsed_time(e1) / 1000.0)
+        lp128 = d_lp128.cpu().numpy()
+        dlp = float(np.abs(lp128 - lp64[sl]).max())
+        dcond = float(np.abs(d_cond128.cpu().numpy() - cond64[sl]).max())
+        S2 = args.c128_samples
+        e0.record(stream)
+        e128.sample_device(d_u[:S2], d_sb[:S2], d_slp[:S2])
+        e1.record(stream)
+        torch.cuda.synchronize()
+        s_per_sample128 = e0.elapsed_time(e1) / 1000.0 / S2
+        same_bits = bool((d_sb[:S2].cpu().numpy() == sbits64[:S2]).all())
+        e128.close()
+        c128 = {"amps_per_s": max_over_ranks(amps128, world) if world == 1 else amps128,
+                "s_per_sample": s_per_sample128, "max_abs_dlog2p_c64_vs_c128": dlp,
+                "max_abs_dcond_c64_vs_c128": dcond, "samples_same_bits_c64_c128": same_bits}
+
+    launches = (ns + 2) * K * A + K   # per string: begin + ns write passes + finish; one item reset per batch
+    out = {
+        "metric": METRIC, "value": value, "unit": "amps/s", "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c64 arena, f64 arithmetic", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n": 70, "width": w["width"], "strings_per_step": A, "mode": "chain",
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
+        "s_per_sample": s_per_sample64, "samples_per_s": world / s_per_sample64,
+        "c128": c128, "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        with tempfile.TemporaryDirectory() as td:
+            plan = os.path.join(td, "plan.txt")
+            open(plan, "w").write(w["plan"])
+            sp = os.path.join(td, "s.txt")
+            open(sp, "w").write("".join(str(int(b)) for b in strings[W * A]) + "\n")
+            cores = os.cpu_count() or 1
+            t, txt, kind = ref_chain_time(plan, sp, cores)
+            ref_lp = float(txt.split()[0])
+            out["cpu_baseline"] = {"value": 1.0 / t, "unit": "amps/s", "cores": cores, "kind": kind,
+                                   "sample": "1 uniform random string of the workload, gsamp2 chain mode (complex64)",
+                                   "abs_dlog2p_vs_gpu_c64": abs(ref_lp - float(lp64[W * A]))}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_gsb(a)

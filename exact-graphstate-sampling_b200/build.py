@@ -1,0 +1,61 @@
+"""Build the executor in-tree: libgsb.so (CUDA, sm_100a) and the gsb2 / gsb2_c128 command lines.
+
+    python build.py [--force]
+
+nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine with the CUDA toolkit.  Outputs sit next
+to this file, where gsb.py loads them.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "libgsb.so")
+CLI = os.path.join(HERE, "gsb2")
+CLI128 = os.path.join(HERE, "gsb2_c128")
+
+NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
+              "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
+LIB_SOURCES = ["gsb_engine.cu", "gsb_plan.cpp", "gsb_order.cpp"]
+LIB_DEPS = LIB_SOURCES + ["gsb_kernels.cuh", "gsb_plan.h"]
+
+
+def _nvcc():
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def _stale(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps)
+
+
+def _run(cmd):
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build(force=False, verbose_ptxas=False):
+    deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(INCLUDE, "gsb.h")]
+    if force or _stale(LIB, deps):
+        cmd = [_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else []) + \
+              ["-shared", "-I" + INCLUDE, "-I" + CSRC, "-o", LIB] + [os.path.join(CSRC, f) for f in LIB_SOURCES]
+        _run(cmd)
+    cli_src = os.path.join(CSRC, "gsb_cli.cpp")
+    if force or _stale(CLI, [cli_src, LIB, os.path.join(INCLUDE, "gsb.h")]):
+        _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + INCLUDE, cli_src, "-L" + HERE, "-lgsb",
+              "-Wl,-rpath,$ORIGIN", "-o", CLI])
+    if not os.path.lexists(CLI128):
+        os.symlink("gsb2", CLI128)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose_ptxas="-v" in sys.argv)

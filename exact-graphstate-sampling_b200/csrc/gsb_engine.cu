@@ -1,0 +1,777 @@
+// libgsb: the C ABI of include/gsb.h on top of the kernels in gsb_kernels.cuh.
+//
+// An engine = one validated plan + one arena (2^R entries) + one stream + device-resident state.  Every mode of the
+// reference executor (gsamp2.cpp:149-225) becomes a sequence of kernel launches per string or sample:
+//   begin (unit table) -> per step [norm pass] write pass -> finish (log2 Pr, next item)
+// with all scalar decisions made on the device.  The per-item sequences of the batch modes are captured once as
+// CUDA graphs and replayed per item; the item index advances on the device, so a batch of strings is one H2D copy,
+// N graph launches and one D2H copy.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "gsb.h"
+#include "gsb_kernels.cuh"
+#include "gsb_plan.h"
+
+namespace gsb {
+
+static thread_local std::string g_err;
+
+static int fail(int code, const std::string &msg) {
+    g_err = msg;
+    return code;
+}
+
+#define GSB_CK(x)                                                                                         \
+    do {                                                                                                  \
+        cudaError_t e_ = (x);                                                                             \
+        if (e_ != cudaSuccess) {                                                                          \
+            return fail(GSB_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #x);    \
+        }                                                                                                 \
+    } while (0)
+
+struct Launch {
+    int grid = 1, block = 1, U = 1, tl = 0, cl = 0;
+    unsigned int nchunks = 1;
+    void *fn = nullptr;
+};
+
+struct DevGuard {
+    int prev = -1;
+    explicit DevGuard(int d) {
+        cudaGetDevice(&prev);
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DevGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <typename E, int NTQ, int M, int U>
+static void *pick_w(bool write) {
+    return write ? (void *)k_step<E, NTQ, M, U, true> : (void *)k_step<E, NTQ, M, U, false>;
+}
+template <typename E, int NTQ, int M>
+static void *pick_u(int U, bool write) {
+    return U == 4 ? pick_w<E, NTQ, M, 4>(write) : pick_w<E, NTQ, M, 1>(write);
+}
+template <typename E, int NTQ>
+static void *pick_m(int m, int U, bool write) {
+    return m == 2 ? pick_u<E, NTQ, 2>(U, write) : pick_u<E, NTQ, 1>(U, write);
+}
+template <typename E>
+static void *pick_step_kernel(int ntq, int m, int U, bool write) {
+    if (ntq == 4) return pick_m<E, 4>(m, U, write);
+    if (ntq == 2) return pick_m<E, 2>(m, U, write);
+    return pick_m<E, 1>(m, U, write);
+}
+
+struct Engine {
+    HPlan plan;
+    int prec = 64, dev = 0, sms = 0;
+    size_t esize = 8;
+    void *mem = nullptr;
+    cudaStream_t stream = nullptr;       // where work is queued (own_stream unless the caller set one)
+    cudaStream_t own_stream = nullptr;
+    DevState *st = nullptr;
+    double *partials = nullptr;
+    int cap = 1024;                      // items per device batch
+    int8_t *d_forced = nullptr, *d_bits = nullptr;
+    double *d_unif = nullptr, *d_cond = nullptr, *d_logp = nullptr, *d_aux = nullptr;
+    void *d_dump = nullptr;
+    size_t dump_bytes = 0;
+    std::vector<StepArgs> args;
+    std::vector<Launch> lw, ln;
+    std::map<int, cudaGraphExec_t> graphs;   // key: graph kind
+    std::map<void *, int> occ;
+
+    ~Engine() {
+        DevGuard g(dev);
+        for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
+        cudaFree(mem);
+        cudaFree(st);
+        cudaFree(partials);
+        cudaFree(d_forced);
+        cudaFree(d_bits);
+        cudaFree(d_unif);
+        cudaFree(d_cond);
+        cudaFree(d_logp);
+        cudaFree(d_aux);
+        cudaFree(d_dump);
+        if (own_stream) cudaStreamDestroy(own_stream);
+    }
+
+    int occupancy(void *fn, int block) {
+        auto it = occ.find(fn);
+        if (it != occ.end()) return it->second;
+        int nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0) != cudaSuccess || nb < 1) nb = 1;
+        occ[fn] = nb;
+        return nb;
+    }
+
+    void *step_fn(int ntq, int m, int U, bool write) const {
+        return prec == 128 ? pick_step_kernel<double2>(ntq, m, U, write) : pick_step_kernel<float2>(ntq, m, U, write);
+    }
+
+    Launch shape(const StepArgs &a, bool write) {
+        Launch L;
+        const uint64_t N = 1ULL << a.nk;
+        // blocks of at least one full warp (the reductions shuffle over 32 lanes); below 32 cosets the threads
+        // tid >= 2^nk idle
+        if (N >= 1024) { L.block = 256; L.U = 4; L.tl = 8; }
+        else if (N >= 256) { L.block = 256; L.U = 1; L.tl = 8; }
+        else { L.block = (int)std::max<uint64_t>(32, N); L.U = 1; L.tl = a.nk; }
+        L.cl = L.tl + (L.U == 4 ? 2 : 0);
+        L.nchunks = (unsigned int)(N >> L.cl);
+        L.fn = step_fn(a.ntq, a.m, L.U, write);
+        const int cap_blocks = occupancy(L.fn, L.block) * sms;
+        L.grid = (int)std::min<uint64_t>(L.nchunks, (uint64_t)cap_blocks);
+        return L;
+    }
+
+    Ctx ctx(int driver, int k1, const Launch &L, bool use_forced, bool use_unif) const {
+        Ctx c;
+        c.st = st;
+        c.partials = partials;
+        c.forced = use_forced ? d_forced : nullptr;
+        c.unif = use_unif ? d_unif : nullptr;
+        c.bits_out = d_bits;
+        c.cond_out = d_cond;
+        c.ns = plan.ns;
+        c.driver = driver;
+        c.k1 = k1;
+        c.tpb_log2 = L.tl;
+        c.chunk_log2 = L.cl;
+        c.nchunks = L.nchunks;
+        return c;
+    }
+
+    cudaError_t launch_step(int k, bool write, int driver, int k1, bool use_forced, bool use_unif) {
+        const Launch &L = write ? lw[(size_t)k] : ln[(size_t)k];
+        StepArgs a = args[(size_t)k];
+        Ctx c = ctx(driver, k1, L, use_forced, use_unif);
+        void *memp = mem;
+        void *kargs[] = {&a, &memp, &c};
+        return cudaLaunchKernel(L.fn, dim3((unsigned)L.grid), dim3((unsigned)L.block), kargs, 0, stream);
+    }
+
+    cudaError_t launch_begin() {
+        if (prec == 128) k_begin<double2><<<1, 1, 0, stream>>>((double2 *)mem, st);
+        else k_begin<float2><<<1, 1, 0, stream>>>((float2 *)mem, st);
+        return cudaGetLastError();
+    }
+
+    // One item: begin, steps k0..k1-1, finish.  driver decides the passes:
+    //   CHAIN: norm + write per step; CHAIN1: write; HYBRID: norm (skipped on device when forced) + write.
+    cudaError_t enqueue_item(int driver, bool use_forced, bool use_unif) {
+        cudaError_t e = launch_begin();
+        if (e != cudaSuccess) return e;
+        for (int k = 0; k < plan.ns; k++) {
+            if (driver != DRV_CHAIN1) {
+                e = launch_step(k, false, driver, plan.ns, use_forced, use_unif);
+                if (e != cudaSuccess) return e;
+            }
+            e = launch_step(k, true, driver, plan.ns, use_forced, use_unif);
+            if (e != cudaSuccess) return e;
+        }
+        k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
+        return cudaGetLastError();
+    }
+
+    int graph(int kind, cudaGraphExec_t *out) {
+        auto it = graphs.find(kind);
+        if (it != graphs.end()) { *out = it->second; return 0; }
+        int driver = kind == 0 ? DRV_CHAIN1 : kind == 3 ? DRV_HYBRID : DRV_CHAIN;
+        bool use_forced = kind != 2, use_unif = kind >= 2;
+        cudaGraph_t g = nullptr;
+        GSB_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = enqueue_item(driver, use_forced, use_unif);
+        cudaError_t e2 = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); GSB_CK(e); }
+        GSB_CK(e2);
+        cudaGraphExec_t ex = nullptr;
+        e = cudaGraphInstantiate(&ex, g, 0);
+        cudaGraphDestroy(g);
+        GSB_CK(e);
+        graphs[kind] = ex;
+        *out = ex;
+        return 0;
+    }
+
+    // Run `n` items of graph `kind` with inputs already in d_forced / d_unif rows 0..n-1.
+    int run_graph_items(int kind, int64_t n) {
+        cudaGraphExec_t ex;
+        int rc = graph(kind, &ex);
+        if (rc) return rc;
+        k_set_item<<<1, 1, 0, stream>>>(st, 0);
+        GSB_CK(cudaGetLastError());
+        for (int64_t i = 0; i < n; i++) GSB_CK(cudaGraphLaunch(ex, stream));
+        return 0;
+    }
+};
+
+static int make_args(Engine &E) {
+    const HPlan &p = E.plan;
+    E.args.resize((size_t)p.ns);
+    for (int k = 0; k < p.ns; k++) {
+        const HStep &s = p.st[(size_t)k];
+        StepArgs a;
+        memset(&a, 0, sizeof a);
+        for (int j = 0; j < s.nk; j++) a.tk[j] = s.tk[(size_t)j];
+        a.ntq = (int)s.tqs.size();
+        for (int i = 0; i < a.ntq; i++) {
+            a.tq[i] = s.tqs[(size_t)i];
+            a.tau0[i] = s.tau0[i];
+            a.tau1[i] = s.tau1[i];
+            a.par[i] = s.par[i];
+        }
+        a.g = s.m == 2 ? s.g : 0;
+        a.rhoc = s.rhoc;
+        for (int b = 0; b < 2; b++)
+            for (int x = 0; x < 2; x++) { a.Mr[b][x] = s.Mr[b][x]; a.Mi[b][x] = s.Mi[b][x]; }
+        a.nk = s.nk;
+        a.k = k;
+        a.m = s.m;
+        E.args[(size_t)k] = a;
+    }
+    size_t maxgrid = 1;
+    E.lw.resize((size_t)p.ns);
+    E.ln.resize((size_t)p.ns);
+    for (int k = 0; k < p.ns; k++) {
+        E.lw[(size_t)k] = E.shape(E.args[(size_t)k], true);
+        E.ln[(size_t)k] = E.shape(E.args[(size_t)k], false);
+        maxgrid = std::max(maxgrid, (size_t)std::max(E.lw[(size_t)k].grid, E.ln[(size_t)k].grid));
+    }
+    maxgrid = std::max(maxgrid, (size_t)E.sms * 8);
+    GSB_CK(cudaMalloc(&E.partials, maxgrid * 2 * sizeof(double)));
+    return 0;
+}
+
+static int open_plan(const char *text, size_t len, int precision, int device, gsb_engine **out) {
+    if (!out) return fail(GSB_E_USAGE, "null output handle");
+    *out = nullptr;
+    if (precision != 64 && precision != 128) return fail(GSB_E_USAGE, "precision must be 64 or 128");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(GSB_E_CUDA, "no CUDA device is visible");
+    if (device < 0 || device >= ndev) return fail(GSB_E_USAGE, "device index out of range");
+    Engine *E = new Engine();
+    E->prec = precision;
+    E->esize = precision == 128 ? 16 : 8;
+    E->dev = device;
+    std::string err;
+    int rc = parse_plan_text(text, len, E->plan, err);
+    if (!rc) rc = validate_plan(E->plan, err);
+    if (rc) { delete E; return fail(rc, err); }
+    DevGuard g(device);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) { delete E; return fail(GSB_E_CUDA, "cudaGetDeviceProperties failed"); }
+    E->sms = prop.multiProcessorCount;
+    auto cuda_fail = [&](cudaError_t e, const char *what) {
+        delete E;
+        return fail(GSB_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    };
+    cudaError_t e = cudaStreamCreateWithFlags(&E->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "stream");
+    E->stream = E->own_stream;
+    const size_t arena = ((size_t)1 << E->plan.R) * E->esize;
+    e = cudaMalloc(&E->mem, arena);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        char b[160];
+        snprintf(b, sizeof b, "allocation of %zu bytes for the 2^%d arena failed", arena, E->plan.R);
+        delete E;
+        return fail(GSB_E_ALLOC, b);
+    }
+    e = cudaMemsetAsync(E->mem, 0, arena, E->stream);
+    if (e != cudaSuccess) return cuda_fail(e, "arena clear");
+    const size_t ns = (size_t)std::max(1, E->plan.ns), cap = (size_t)E->cap;
+    if ((e = cudaMalloc(&E->st, sizeof(DevState))) != cudaSuccess) return cuda_fail(e, "state");
+    if ((e = cudaMemsetAsync(E->st, 0, sizeof(DevState), E->stream)) != cudaSuccess) return cuda_fail(e, "state");
+    if ((e = cudaMalloc(&E->d_forced, cap * ns)) != cudaSuccess) return cuda_fail(e, "buffers");
+    if ((e = cudaMalloc(&E->d_bits, cap * ns)) != cudaSuccess) return cuda_fail(e, "buffers");
+    if ((e = cudaMalloc(&E->d_unif, cap * ns * 8)) != cudaSuccess) return cuda_fail(e, "buffers");
+    if ((e = cudaMalloc(&E->d_cond, cap * ns * 8)) != cudaSuccess) return cuda_fail(e, "buffers");
+    if ((e = cudaMalloc(&E->d_logp, cap * 8)) != cudaSuccess) return cuda_fail(e, "buffers");
+    if ((e = cudaMalloc(&E->d_aux, cap * 8)) != cudaSuccess) return cuda_fail(e, "buffers");
+    if ((e = cudaMemsetAsync(E->d_forced, 0, cap * ns, E->stream)) != cudaSuccess) return cuda_fail(e, "buffers");
+    rc = make_args(*E);
+    if (rc) { std::string m = g_err; delete E; return fail(rc, m); }
+    if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return cuda_fail(e, "set-up");
+    *out = reinterpret_cast<gsb_engine *>(E);
+    return 0;
+}
+
+static Engine *eng(gsb_engine *e) { return reinterpret_cast<Engine *>(e); }
+static const Engine *eng(const gsb_engine *e) { return reinterpret_cast<const Engine *>(e); }
+
+// uniforms of one 'sample'/'sample2' stream item: one draw per step, in step order (gsamp2.cpp:46-47,151,159-160)
+static void sample_uniforms(int seeding, uint64_t seed, uint64_t i, int ns, double *u) {
+    std::uniform_real_distribution<double> U(0, 1);
+    if (seeding == GSB_SEED_SEQ) {
+        std::seed_seq sq{(unsigned)(seed & 0xffffffffu), (unsigned)(seed >> 32), (unsigned)(i & 0xffffffffu),
+                         (unsigned)(i >> 32), 0x9E3779B9u};
+        std::mt19937_64 rng(sq);
+        for (int k = 0; k < ns; k++) u[k] = U(rng);
+    } else {
+        std::mt19937_64 rng(seed + i);
+        for (int k = 0; k < ns; k++) u[k] = U(rng);
+    }
+}
+
+// uniforms of a hybrid / resume line: one draw per '?' step from k0 on, in step order (gsamp2.cpp:86, 206, 215)
+static void free_uniforms(uint64_t seed, const int8_t *forced, int k0, int ns, double *u) {
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> U(0, 1);
+    for (int k = 0; k < ns; k++) u[k] = 0;
+    for (int k = k0; k < ns; k++)
+        if (forced[k] < 0) u[k] = U(rng);
+}
+
+}  // namespace gsb
+
+using namespace gsb;
+
+extern "C" {
+
+const char *gsb_version(void) { return "gsb 0.1 (sm_100a)"; }
+const char *gsb_last_error(void) { return g_err.c_str(); }
+
+int gsb_open_text(const char *plan_text, size_t len, int precision, int device, gsb_engine **out) {
+    if (!plan_text) return fail(GSB_E_USAGE, "null plan text");
+    return open_plan(plan_text, len, precision, device, out);
+}
+
+int gsb_validate_text(const char *plan_text, size_t len, int *n, int *nsteps, int *R) {
+    if (!plan_text) return fail(GSB_E_USAGE, "null plan text");
+    HPlan p;
+    std::string err;
+    int rc = parse_plan_text(plan_text, len, p, err);
+    if (!rc) rc = validate_plan(p, err);
+    if (rc) return fail(rc, err);
+    if (n) *n = p.n;
+    if (nsteps) *nsteps = p.ns;
+    if (R) *R = p.R;
+    return 0;
+}
+
+int gsb_open_file(const char *plan_path, int precision, int device, gsb_engine **out) {
+    if (!plan_path) return fail(GSB_E_USAGE, "null plan path");
+    FILE *f = fopen(plan_path, "rb");
+    if (!f) return fail(GSB_E_PLAN_HEADER, std::string("cannot open plan ") + plan_path);
+    std::string text;
+    char buf[1 << 16];
+    size_t n;
+    while ((n = fread(buf, 1, sizeof buf, f)) > 0) text.append(buf, n);
+    fclose(f);
+    return open_plan(text.data(), text.size(), precision, device, out);
+}
+
+int gsb_close(gsb_engine *e) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    delete eng(e);
+    return 0;
+}
+
+int gsb_info(const gsb_engine *e, int *n, int *nsteps, int *R, int *precision) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    const Engine *E = eng(e);
+    if (n) *n = E->plan.n;
+    if (nsteps) *nsteps = E->plan.ns;
+    if (R) *R = E->plan.R;
+    if (precision) *precision = E->prec;
+    return 0;
+}
+
+int gsb_step_vertices(const gsb_engine *e, int *out) {
+    if (!e || !out) return fail(GSB_E_USAGE, "null argument");
+    const Engine *E = eng(e);
+    for (int k = 0; k < E->plan.ns; k++) out[k] = E->plan.st[(size_t)k].v;
+    return 0;
+}
+
+static int check_bits(const int8_t *b, int64_t n, int ns, bool allow_free) {
+    for (int64_t i = 0; i < n * ns; i++)
+        if (!(b[i] == 0 || b[i] == 1 || (allow_free && b[i] == -1)))
+            return fail(GSB_E_USAGE, allow_free ? "bits must be 0, 1 or -1" : "bits must be 0 or 1");
+    return 0;
+}
+
+// forced-string batch through graph `kind` (0 chain, 1 prob)
+static int forced_batch(Engine *E, int kind, const int8_t *bits, int64_t nstr, double *log2p, double *cond) {
+    const int ns = E->plan.ns;
+    for (int64_t off = 0; off < nstr; off += E->cap) {
+        const int64_t nb = std::min<int64_t>(E->cap, nstr - off);
+        if (ns) GSB_CK(cudaMemcpyAsync(E->d_forced, bits + off * ns, (size_t)(nb * ns), cudaMemcpyHostToDevice, E->stream));
+        int rc = E->run_graph_items(kind, nb);
+        if (rc) return rc;
+        if (log2p) GSB_CK(cudaMemcpyAsync(log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToHost, E->stream));
+        if (cond && ns) GSB_CK(cudaMemcpyAsync(cond + off * ns, E->d_cond, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToHost, E->stream));
+        GSB_CK(cudaStreamSynchronize(E->stream));
+    }
+    return 0;
+}
+
+int gsb_prob(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (nstr < 0 || (nstr && (!bits || !log2p))) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    int rc = check_bits(bits, nstr, E->plan.ns, false);
+    if (rc) return rc;
+    return forced_batch(E, 1, bits, nstr, log2p, nullptr);
+}
+
+int gsb_chain(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p, double *cond) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (nstr < 0 || (nstr && (!bits || !log2p))) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    int rc = check_bits(bits, nstr, E->plan.ns, false);
+    if (rc) return rc;
+    return forced_batch(E, 0, bits, nstr, log2p, cond);
+}
+
+static int uniform_batch(Engine *E, const double *u, int64_t count, int8_t *bits, double *log2p) {
+    const int ns = E->plan.ns;
+    for (int64_t off = 0; off < count; off += E->cap) {
+        const int64_t nb = std::min<int64_t>(E->cap, count - off);
+        if (ns) GSB_CK(cudaMemcpyAsync(E->d_unif, u + off * ns, (size_t)(nb * ns) * 8, cudaMemcpyHostToDevice, E->stream));
+        int rc = E->run_graph_items(2, nb);
+        if (rc) return rc;
+        if (log2p) GSB_CK(cudaMemcpyAsync(log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToHost, E->stream));
+        if (bits && ns) GSB_CK(cudaMemcpyAsync(bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToHost, E->stream));
+        GSB_CK(cudaStreamSynchronize(E->stream));
+    }
+    return 0;
+}
+
+int gsb_sample_uniform(gsb_engine *e, const double *u, int64_t count, int8_t *bits, double *log2p) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (count < 0 || (count && (!u || !bits || !log2p))) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    return uniform_batch(E, u, count, bits, log2p);
+}
+
+int gsb_sample(gsb_engine *e, int seeding, uint64_t seed, int64_t first, int64_t count, int8_t *bits, double *log2p) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (seeding != GSB_SEED_INT && seeding != GSB_SEED_SEQ) return fail(GSB_E_USAGE, "unknown seeding");
+    if (count < 0 || first < 0 || (count && (!bits || !log2p))) return fail(GSB_E_USAGE, "bad argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    const int ns = E->plan.ns;
+    std::vector<double> u((size_t)std::max<int64_t>(1, std::min<int64_t>(count, E->cap)) * (size_t)std::max(ns, 1));
+    for (int64_t off = 0; off < count; off += E->cap) {
+        const int64_t nb = std::min<int64_t>(E->cap, count - off);
+        for (int64_t i = 0; i < nb; i++) sample_uniforms(seeding, seed, (uint64_t)(first + off + i), ns, u.data() + i * ns);
+        int rc = uniform_batch(E, u.data(), nb, bits + off * ns, log2p + off);
+        if (rc) return rc;
+    }
+    return 0;
+}
+
+int gsb_hybrid(gsb_engine *e, const int8_t *forced, int64_t nstr, uint64_t seed, int64_t first_line, int8_t *bits,
+               double *log2p, double *cond) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (nstr < 0 || (nstr && (!forced || !bits || !log2p))) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    const int ns = E->plan.ns;
+    int rc = check_bits(forced, nstr, ns, true);
+    if (rc) return rc;
+    std::vector<double> u((size_t)std::max<int64_t>(1, std::min<int64_t>(nstr, E->cap)) * (size_t)std::max(ns, 1));
+    for (int64_t off = 0; off < nstr; off += E->cap) {
+        const int64_t nb = std::min<int64_t>(E->cap, nstr - off);
+        for (int64_t i = 0; i < nb; i++)
+            free_uniforms(seed + (uint64_t)(first_line + off + i), forced + (off + i) * ns, 0, ns, u.data() + i * ns);
+        if (ns) {
+            GSB_CK(cudaMemcpyAsync(E->d_forced, forced + off * ns, (size_t)(nb * ns), cudaMemcpyHostToDevice, E->stream));
+            GSB_CK(cudaMemcpyAsync(E->d_unif, u.data(), (size_t)(nb * ns) * 8, cudaMemcpyHostToDevice, E->stream));
+        }
+        rc = E->run_graph_items(3, nb);
+        if (rc) return rc;
+        GSB_CK(cudaMemcpyAsync(log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToHost, E->stream));
+        if (ns) GSB_CK(cudaMemcpyAsync(bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToHost, E->stream));
+        if (cond && ns) GSB_CK(cudaMemcpyAsync(cond + off * ns, E->d_cond, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToHost, E->stream));
+        GSB_CK(cudaStreamSynchronize(E->stream));
+    }
+    return 0;
+}
+
+int gsb_dump_shape(const gsb_engine *e, int K, int *nk, int *ntq) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    const Engine *E = eng(e);
+    if (K < 0) return fail(GSB_E_USAGE, "K must be >= 0");
+    if (K >= E->plan.ns) {
+        if (nk) *nk = 0;
+        if (ntq) *ntq = 1;
+    } else {
+        if (nk) *nk = E->plan.st[(size_t)K].nk;
+        if (ntq) *ntq = (int)E->plan.st[(size_t)K].tqs.size();
+    }
+    return 0;
+}
+
+static StepArgs dump_args(const Engine *E, int K) {
+    if (K < E->plan.ns) return E->args[(size_t)K];
+    StepArgs a;
+    memset(&a, 0, sizeof a);
+    a.ntq = 1;
+    return a;
+}
+
+static int ensure_dump(Engine *E, size_t bytes) {
+    if (E->dump_bytes >= bytes) return 0;
+    cudaFree(E->d_dump);
+    E->d_dump = nullptr;
+    E->dump_bytes = 0;
+    cudaError_t e = cudaMalloc(&E->d_dump, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return fail(GSB_E_ALLOC, "allocation of the dump buffer failed"); }
+    E->dump_bytes = bytes;
+    return 0;
+}
+
+int gsb_prefix(gsb_engine *e, const int8_t *forced, int K, void *dump, double *logscale, double *log2p_prefix) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    const int ns = E->plan.ns;
+    if (!forced || !dump || K < 0) return fail(GSB_E_USAGE, "bad argument");
+    for (int k = 0; k < std::min(K, ns); k++)
+        if (forced[k] < 0) return fail(GSB_E_PREFIX_FREE, "'?' before K in prefix mode");
+        else if (forced[k] > 1) return fail(GSB_E_USAGE, "bits must be 0 or 1");
+    DevGuard g(E->dev);
+    const int Kr = std::min(K, ns);
+    std::vector<int8_t> row((size_t)std::max(ns, 1), 0);
+    for (int k = 0; k < Kr; k++) row[(size_t)k] = forced[k];
+    if (ns) GSB_CK(cudaMemcpyAsync(E->d_forced, row.data(), (size_t)ns, cudaMemcpyHostToDevice, E->stream));
+    k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
+    GSB_CK(E->launch_begin());
+    for (int k = 0; k < Kr; k++) GSB_CK(E->launch_step(k, true, DRV_HYBRID, Kr, true, false));
+    int nk, ntq;
+    gsb_dump_shape(e, K, &nk, &ntq);
+    const size_t nent = ((size_t)1 << nk) * (size_t)ntq, bytes = nent * E->esize;
+    int rc = ensure_dump(E, bytes);
+    if (rc) return rc;
+    StepArgs a = dump_args(E, K);
+    const int grid = (int)std::min<size_t>((nent + 255) / 256, (size_t)E->sms * 8);
+    if (E->prec == 128) k_gather<double2><<<grid, 256, 0, E->stream>>>(a, (const double2 *)E->mem, ntq, (double2 *)E->d_dump);
+    else k_gather<float2><<<grid, 256, 0, E->stream>>>(a, (const float2 *)E->mem, ntq, (float2 *)E->d_dump);
+    GSB_CK(cudaGetLastError());
+    GSB_CK(cudaMemcpyAsync(dump, E->d_dump, bytes, cudaMemcpyDeviceToHost, E->stream));
+    DevState hs;
+    GSB_CK(cudaMemcpyAsync(&hs, E->st, sizeof hs, cudaMemcpyDeviceToHost, E->stream));
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    if (logscale) *logscale = hs.logscale;
+    if (log2p_prefix) *log2p_prefix = hs.logp;
+    return 0;
+}
+
+int gsb_resume(gsb_engine *e, const int8_t *forced, int K, uint64_t seed, int64_t line, int nslices,
+               const void *const *dumps, const double *logscales, const uint64_t *cshift, const uint64_t *tqshift,
+               int8_t *bits, double *log2p_full, double *log2p_prefix, double *cond) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    const int ns = E->plan.ns;
+    if (!forced || !dumps || !logscales || !bits || !log2p_full || nslices < 1 || K < 0) return fail(GSB_E_USAGE, "bad argument");
+    for (int s = 0; s < nslices; s++)
+        if (!dumps[s]) return fail(GSB_E_DUMP_MISSING, "missing dump table");
+    int rc = check_bits(forced, 1, ns, true);
+    if (rc) return rc;
+    DevGuard g(E->dev);
+    int nk, ntq;
+    gsb_dump_shape(e, K, &nk, &ntq);
+    const StepArgs a = dump_args(E, K);
+    // twist translation (gsamp2.cpp:184-195)
+    std::vector<uint64_t> cs((size_t)nslices, 0);
+    std::vector<int> tperm((size_t)nslices * 4, 0);
+    for (int s = 0; s < nslices; s++) {
+        if (cshift) {
+            if (cshift[s] >> nk) return fail(GSB_E_TWIST_RANGE, "twist cshift exceeds the kept coordinates");
+            cs[(size_t)s] = cshift[s];
+        }
+        for (int t = 0; t < ntq; t++) {
+            int pos = t;
+            if (tqshift) {
+                pos = -1;
+                for (int u = 0; u < ntq; u++)
+                    if (a.tq[u] == (a.tq[t] ^ tqshift[s])) pos = u;
+                if (pos < 0) return fail(GSB_E_TWIST_RANGE, "twist tqshift does not map the coset offsets of step K onto themselves");
+            }
+            tperm[(size_t)s * 4 + (size_t)t] = pos;
+        }
+    }
+    double L = -1e300;
+    for (int s = 0; s < nslices; s++) L = std::max(L, logscales[s]);
+    std::vector<double> f((size_t)nslices);
+    for (int s = 0; s < nslices; s++) f[(size_t)s] = std::exp2(logscales[s] - L);
+    const size_t nent = ((size_t)1 << nk) * (size_t)ntq, tbytes = nent * E->esize;
+    // device copies: slice tables back to back, then the small arrays
+    rc = ensure_dump(E, tbytes * (size_t)nslices);
+    if (rc) return rc;
+    std::vector<const void *> dptr((size_t)nslices);
+    for (int s = 0; s < nslices; s++) {
+        dptr[(size_t)s] = (const char *)E->d_dump + tbytes * (size_t)s;
+        GSB_CK(cudaMemcpyAsync((void *)dptr[(size_t)s], dumps[s], tbytes, cudaMemcpyHostToDevice, E->stream));
+    }
+    void *small = nullptr;
+    const size_t sbytes = (size_t)nslices * (8 + 8 + 8 + 16);
+    GSB_CK(cudaMallocAsync(&small, sbytes, E->stream));
+    char *sp = (char *)small;
+    GSB_CK(cudaMemcpyAsync(sp, dptr.data(), (size_t)nslices * 8, cudaMemcpyHostToDevice, E->stream));
+    GSB_CK(cudaMemcpyAsync(sp + (size_t)nslices * 8, f.data(), (size_t)nslices * 8, cudaMemcpyHostToDevice, E->stream));
+    GSB_CK(cudaMemcpyAsync(sp + (size_t)nslices * 16, cs.data(), (size_t)nslices * 8, cudaMemcpyHostToDevice, E->stream));
+    GSB_CK(cudaMemcpyAsync(sp + (size_t)nslices * 24, tperm.data(), (size_t)nslices * 16, cudaMemcpyHostToDevice, E->stream));
+    ResumeArgs ra;
+    ra.dumps = (const void *const *)sp;
+    ra.f = (const double *)(sp + (size_t)nslices * 8);
+    ra.cshift = (const uint64_t *)(sp + (size_t)nslices * 16);
+    ra.tperm = (const int *)(sp + (size_t)nslices * 24);
+    ra.nsl = nslices;
+    ra.ntq = ntq;
+    ra.K = K;
+    ra.L = L;
+    // forced row and the uniforms of the '?' steps (mt19937_64(seed + line), gsamp2.cpp:206)
+    std::vector<int8_t> row((size_t)std::max(ns, 1), 0);
+    for (int k = 0; k < ns; k++) row[(size_t)k] = forced[k];
+    std::vector<double> u((size_t)std::max(ns, 1), 0.0);
+    if (ns) free_uniforms(seed + (uint64_t)line, row.data(), std::min(K, ns), ns, u.data());
+    if (ns) {
+        GSB_CK(cudaMemcpyAsync(E->d_forced, row.data(), (size_t)ns, cudaMemcpyHostToDevice, E->stream));
+        GSB_CK(cudaMemcpyAsync(E->d_unif, u.data(), (size_t)ns * 8, cudaMemcpyHostToDevice, E->stream));
+    }
+    k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
+    const uint64_t Nc = 1ULL << nk;
+    Launch L1;
+    L1.block = (int)std::max<uint64_t>(32, std::min<uint64_t>(256, Nc));
+    Ctx c = E->ctx(DRV_HYBRID, ns, L1, true, true);
+    const int grid = (int)std::min<uint64_t>((Nc + 255) / 256, (uint64_t)E->sms * 8);
+    if (E->prec == 128) k_resume_sum<double2><<<grid, L1.block, 0, E->stream>>>(a, (double2 *)E->mem, ra, c);
+    else k_resume_sum<float2><<<grid, L1.block, 0, E->stream>>>(a, (float2 *)E->mem, ra, c);
+    GSB_CK(cudaGetLastError());
+    for (int k = K; k < ns; k++) {
+        GSB_CK(E->launch_step(k, false, DRV_HYBRID, ns, true, true));
+        GSB_CK(E->launch_step(k, true, DRV_HYBRID, ns, true, true));
+    }
+    DevState hs;
+    GSB_CK(cudaMemcpyAsync(&hs, E->st, sizeof hs, cudaMemcpyDeviceToHost, E->stream));
+    std::vector<int8_t> hb((size_t)std::max(ns, 1), 0);
+    std::vector<double> hc((size_t)std::max(ns, 1), 0.0);
+    if (ns) {
+        GSB_CK(cudaMemcpyAsync(hb.data(), E->d_bits, (size_t)ns, cudaMemcpyDeviceToHost, E->stream));
+        GSB_CK(cudaMemcpyAsync(hc.data(), E->d_cond, (size_t)ns * 8, cudaMemcpyDeviceToHost, E->stream));
+    }
+    GSB_CK(cudaFreeAsync(small, E->stream));
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    for (int k = 0; k < ns; k++) bits[k] = k < K ? forced[k] : hb[(size_t)k];
+    if (cond)
+        for (int k = K; k < ns; k++) cond[k] = hc[(size_t)k];
+    *log2p_full = hs.aux + hs.logp;
+    if (log2p_prefix) *log2p_prefix = hs.aux;
+    return 0;
+}
+
+int gsb_chain_device(gsb_engine *e, const int8_t *d_bits, int64_t nstr, double *d_log2p, double *d_cond) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (nstr < 0 || (nstr && (!d_bits || !d_log2p))) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    const int ns = E->plan.ns;
+    for (int64_t off = 0; off < nstr; off += E->cap) {
+        const int64_t nb = std::min<int64_t>(E->cap, nstr - off);
+        if (ns) GSB_CK(cudaMemcpyAsync(E->d_forced, d_bits + off * ns, (size_t)(nb * ns), cudaMemcpyDeviceToDevice, E->stream));
+        int rc = E->run_graph_items(0, nb);
+        if (rc) return rc;
+        GSB_CK(cudaMemcpyAsync(d_log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToDevice, E->stream));
+        if (d_cond && ns) GSB_CK(cudaMemcpyAsync(d_cond + off * ns, E->d_cond, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToDevice, E->stream));
+    }
+    return 0;
+}
+
+int gsb_sample_device(gsb_engine *e, const double *d_u, int64_t count, int8_t *d_bits, double *d_log2p) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (count < 0 || (count && (!d_u || !d_bits || !d_log2p))) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    const int ns = E->plan.ns;
+    for (int64_t off = 0; off < count; off += E->cap) {
+        const int64_t nb = std::min<int64_t>(E->cap, count - off);
+        if (ns) GSB_CK(cudaMemcpyAsync(E->d_unif, d_u + off * ns, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToDevice, E->stream));
+        int rc = E->run_graph_items(2, nb);
+        if (rc) return rc;
+        GSB_CK(cudaMemcpyAsync(d_log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToDevice, E->stream));
+        if (ns) GSB_CK(cudaMemcpyAsync(d_bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToDevice, E->stream));
+    }
+    return 0;
+}
+
+int gsb_synchronize(gsb_engine *e) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    return 0;
+}
+
+int gsb_set_stream(gsb_engine *e, void *cuda_stream) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    E->stream = cuda_stream ? (cudaStream_t)cuda_stream : E->own_stream;
+    return 0;
+}
+
+int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_write, float *ms_norm) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (!bits || !ms_write || (mode != 0 && mode != 1)) return fail(GSB_E_USAGE, "bad argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    const int ns = E->plan.ns;
+    int rc = check_bits(bits, 1, ns, false);
+    if (rc) return rc;
+    const int driver = mode == 0 ? DRV_CHAIN1 : DRV_CHAIN;
+    std::vector<cudaEvent_t> ev((size_t)(2 * ns + 1));
+    for (auto &x : ev) GSB_CK(cudaEventCreate(&x));
+    if (ns) GSB_CK(cudaMemcpyAsync(E->d_forced, bits, (size_t)ns, cudaMemcpyHostToDevice, E->stream));
+    k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
+    GSB_CK(E->launch_begin());
+    GSB_CK(cudaEventRecord(ev[0], E->stream));
+    for (int k = 0; k < ns; k++) {
+        if (driver == DRV_CHAIN) GSB_CK(E->launch_step(k, false, driver, ns, true, false));
+        GSB_CK(cudaEventRecord(ev[(size_t)(2 * k + 1)], E->stream));
+        GSB_CK(E->launch_step(k, true, driver, ns, true, false));
+        GSB_CK(cudaEventRecord(ev[(size_t)(2 * k + 2)], E->stream));
+    }
+    k_finish<<<1, 1, 0, E->stream>>>(E->st, E->d_logp, E->d_aux, driver, ns);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    for (int k = 0; k < ns; k++) {
+        float a = 0, b = 0;
+        GSB_CK(cudaEventElapsedTime(&a, ev[(size_t)(2 * k)], ev[(size_t)(2 * k + 1)]));
+        GSB_CK(cudaEventElapsedTime(&b, ev[(size_t)(2 * k + 1)], ev[(size_t)(2 * k + 2)]));
+        if (ms_norm) ms_norm[k] = driver == DRV_CHAIN ? a : 0.f;
+        ms_write[k] = b;
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+    return 0;
+}
+
+int gsb_launches_per_item(const gsb_engine *e, int mode, int64_t *launches) {
+    if (!e || !launches) return fail(GSB_E_USAGE, "null argument");
+    const Engine *E = eng(e);
+    const int64_t ns = E->plan.ns;
+    *launches = mode == 0 ? ns + 2 : 2 * ns + 2;
+    return 0;
+}
+
+}  // extern "C"

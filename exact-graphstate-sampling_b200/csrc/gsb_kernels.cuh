@@ -1,0 +1,417 @@
+// Device side of the in-place cut-rank DP executor for sm_100a.
+//
+// One DP step is one streaming pass over the live part of the 2^R arena (reference gsamp2.cpp:39-120, whose
+// `outputs` gsamp2.cpp:32-38 is the per-coset arithmetic):
+//   for every coset c < 2^nk:  base = XOR_{j in c} Tkeep[j]
+//       v_i  = mem[base ^ tq_i]                                  (the 2^q slots of the coset, q <= 2)
+//       S0[tau0_i] += v_i;  S1[tau1_i] += (-1)^(parity(c & rhoc) ^ par_i) v_i     (x = 0 / x = 1 terms)
+//       out[b][tau] = M[b][0] S0[tau] + M[b][1] S1[tau]
+//   norm pass : n_b += sum_tau |out[b][tau]|^2
+//   write pass: mem[base] = sc out[bv][0];  if m = 2: mem[base ^ g] = sc out[bv][1];   nb += |written|^2
+// Each coset reads and overwrites only its own slots, so the pass is race-free with one thread per coset.
+//
+// Layout of a launch: a block covers chunks of 2^chunk_log2 consecutive cosets; thread t handles cosets
+// chunk_base + t + u * blockDim (u < U).  In planner layouts the low coset bits map to the low arena bits
+// (Tkeep[j] = 2^j), so for every offset tq a warp's 32 loads fall in one aligned segment (XOR with a constant only
+// permutes lanes inside it): fully coalesced 256 B (complex64) or 512 B (complex128) per warp access.
+//
+// Reductions are deterministic: per-thread FP64 sums in coset order, a fixed warp-shuffle and block tree, one
+// partial per block, and the last block to finish sums the partials in block order.  That block also runs the
+// scalar step logic of the chosen mode (bit draw, scale, conditional, log2 Pr) on the device, so a whole string
+// or sample runs without a host round trip (the reference's GPU port copies an accumulator back every step,
+// gsamp_cuda.cu:74-83).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace gsb {
+
+enum Driver : int {
+    DRV_CHAIN = 0,   // normalised: norm pass, draw/force, write with 1/sqrt(n_b)      (gsamp2.cpp:39-55)
+    DRV_CHAIN1 = 1,  // one pass, unnormalised storage, cond = nb / (2 prev)         (gsamp2.cpp:59-70)
+    DRV_HYBRID = 2,  // lazily rescaled run_steps: optional norm pass, write with 1/sqrt(prev)   (gsamp2.cpp:77-98)
+};
+
+struct StepArgs {
+    uint64_t tk[40];        // Tkeep (entries >= nk are 0)
+    uint64_t tq[4];         // distinct coset offsets, ascending
+    uint64_t g, rhoc;
+    double Mr[2][2], Mi[2][2];
+    int nk, k, ntq, m;
+    int tau0[4], tau1[4], par[4];
+};
+
+struct DevState {
+    double prev;      // norm of the stored table
+    double lsc;       // CHAIN1: stored amplitudes = true amplitudes * 2^-lsc
+    double logscale;  // HYBRID: the reference's running logscale
+    double logp;      // running log2 probability
+    double sc;        // scale of the next write (CHAIN: 1/sqrt(n_b); CHAIN1: 2^-ek)
+    double n0, n1;    // last norm pass
+    double aux;       // resume: log2 Pr(prefix)
+    int ek;           // CHAIN1: exponent of the next write's power-of-two scale
+    int bv;           // bit of the next write
+    int dead;         // a zero-probability branch was taken: later passes do nothing
+    int item;         // index of the string / sample being evaluated
+    unsigned int counter;   // blocks finished in the current launch
+    int pad;
+};
+
+struct Ctx {
+    DevState *st;
+    double *partials;        // [gridDim][2]
+    const int8_t *forced;    // [cap][ns] or null
+    const double *unif;      // [cap][ns] or null
+    int8_t *bits_out;        // [cap][ns]
+    double *cond_out;        // [cap][ns]
+    int ns;
+    int driver;
+    int k1;                  // end of the step range of this run (HYBRID zero-fill)
+    int tpb_log2;            // log2 blockDim
+    int chunk_log2;          // log2 cosets per chunk (= tpb_log2 + log2 U)
+    unsigned int nchunks;
+};
+
+__device__ __forceinline__ void load_entry(const float2 *p, double &re, double &im) {
+    const float2 v = *p;
+    re = v.x;
+    im = v.y;
+}
+__device__ __forceinline__ void load_entry(const double2 *p, double &re, double &im) {
+    const double2 v = *p;
+    re = v.x;
+    im = v.y;
+}
+__device__ __forceinline__ void store_entry(float2 *p, double re, double im) { *p = make_float2((float)re, (float)im); }
+__device__ __forceinline__ void store_entry(double2 *p, double re, double im) { *p = make_double2(re, im); }
+
+// XOR of tks[j] over the set bits j of c (c may have bits up to 39)
+__device__ __forceinline__ uint64_t xor_cols(const uint64_t *tks, uint64_t c) {
+    uint64_t a = 0;
+    while (c) {
+        const int j = __ffsll((long long)c) - 1;
+        a ^= tks[j];
+        c &= c - 1;
+    }
+    return a;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of (a0, a1) into partials[blockIdx]; returns true in thread 0 of the last block to finish, with
+// the grid totals in (t0, t1).  All threads of the block must call it.
+__device__ __forceinline__ bool grid_reduce2(double a0, double a1, const Ctx &cx, double &t0, double &t1) {
+    __shared__ double red[2][32];
+    __shared__ int last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    a0 = warp_sum(a0);
+    a1 = warp_sum(a1);
+    if (lane == 0) { red[0][warp] = a0; red[1][warp] = a1; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s0 = 0, s1 = 0;
+        for (int w = 0; w < nw; w++) { s0 += red[0][w]; s1 += red[1][w]; }
+        cx.partials[2 * blockIdx.x] = s0;
+        cx.partials[2 * blockIdx.x + 1] = s1;
+        __threadfence();
+        const unsigned int done = atomicAdd(&cx.st->counter, 1u);
+        last = (done == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    // the last block sums the partials in block order: thread t takes blocks t, t + blockDim, ... then a fixed tree
+    double s0 = 0, s1 = 0;
+    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+        s0 += __ldcg(cx.partials + 2 * b);
+        s1 += __ldcg(cx.partials + 2 * b + 1);
+    }
+    s0 = warp_sum(s0);
+    s1 = warp_sum(s1);
+    __syncthreads();
+    if (lane == 0) { red[0][warp] = s0; red[1][warp] = s1; }
+    __syncthreads();
+    if (threadIdx.x != 0) return false;
+    t0 = 0;
+    t1 = 0;
+    for (int w = 0; w < nw; w++) { t0 += red[0][w]; t1 += red[1][w]; }
+    cx.st->counter = 0;
+    return true;
+}
+
+// Scalar logic after a norm pass (one thread).
+__device__ __forceinline__ void norm_epilogue(const Ctx &cx, int k, double n0, double n1) {
+    DevState *st = cx.st;
+    st->n0 = n0;
+    st->n1 = n1;
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    if (cx.driver == DRV_CHAIN) {
+        const double p1 = n1 / (n0 + n1);
+        int bv;
+        if (cx.forced) bv = cx.forced[row + k];
+        else bv = cx.unif[row + k] < p1;
+        const double pb = bv ? p1 : 1 - p1;
+        if (pb <= 0) {
+            st->dead = 1;
+            st->logp = -INFINITY;
+            for (int j = k; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
+            return;
+        }
+        st->logp += log2(pb);
+        cx.bits_out[row + k] = (int8_t)bv;
+        st->bv = bv;
+        st->sc = 1.0 / sqrt(bv ? n1 : n0);
+    } else {   // DRV_HYBRID, a '?' step
+        st->bv = cx.unif[row + k] < n1 / (n0 + n1);
+    }
+}
+
+// Scalar logic after a write pass (one thread).
+__device__ __forceinline__ void write_epilogue(const Ctx &cx, int k, int bv, double nb) {
+    DevState *st = cx.st;
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    if (cx.driver == DRV_CHAIN) {
+        st->prev = nb;
+    } else if (cx.driver == DRV_CHAIN1) {
+        // the write scaled by 2^-ek; the conditional is scale free: nb_true / (2 prev_true)
+        cx.cond_out[row + k] = ldexp(nb, 2 * st->ek) / (2 * st->prev);
+        st->lsc += st->ek;
+        st->prev = nb;
+        if (nb <= 0) {
+            for (int j = k; j < cx.ns; j++) cx.cond_out[row + j] = 0;
+            st->dead = 1;
+            st->logp = -INFINITY;
+            return;
+        }
+        int ex;
+        frexp(nb, &ex);                      // nb = f 2^ex, f in [0.5, 1)
+        st->ek = (ex - 1) >> 1;              // next write scales by 2^-ek: the stored norm stays near 1
+        st->sc = ldexp(1.0, -st->ek);
+    } else {   // DRV_HYBRID
+        const double prev = st->prev;
+        st->logscale += 0.5 * log2(prev);
+        const double c = nb / 2;
+        cx.cond_out[row + k] = c;
+        cx.bits_out[row + k] = (int8_t)bv;
+        st->prev = nb;
+        if (nb <= 0) {
+            for (int j = k; j < cx.k1; j++) {
+                cx.cond_out[row + j] = 0;
+                const int f = cx.forced[row + j];
+                cx.bits_out[row + j] = (int8_t)(f < 0 ? 0 : f);
+            }
+            st->dead = 1;
+            st->logp = -INFINITY;
+            return;
+        }
+        st->logp += log2(c);
+    }
+}
+
+template <typename E, int NTQ, int MOUT, int U, bool WRITE>
+__global__ void __launch_bounds__(256) k_step(const StepArgs s, E *__restrict__ mem, const Ctx cx) {
+    DevState *st = cx.st;
+    if (*(volatile int *)&st->dead) return;
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    int bv = 0;
+    double sc = 1.0;
+    if (WRITE) {
+        if (cx.driver == DRV_HYBRID) {
+            const int f = cx.forced[row + s.k];
+            bv = f >= 0 ? f : st->bv;
+            sc = 1.0 / sqrt(st->prev);
+        } else if (cx.driver == DRV_CHAIN1) {
+            bv = cx.forced[row + s.k];
+            sc = st->sc;
+        } else {
+            bv = st->bv;
+            sc = st->sc;
+        }
+    } else if (cx.driver == DRV_HYBRID && cx.forced[row + s.k] >= 0) {
+        return;   // forced step of a hybrid run: no norm pass (uniform across the grid)
+    }
+
+    __shared__ uint64_t tks[40];
+    for (int j = threadIdx.x; j < 40; j += blockDim.x) tks[j] = s.tk[j];
+    __syncthreads();
+
+    const int tid = threadIdx.x;
+    const int tl = cx.tpb_log2;
+    uint64_t Tt = 0;
+    for (int j = 0; j < tl; j++)
+        if ((tid >> j) & 1) Tt ^= tks[j];
+    const int pt = __popcll((unsigned long long)tid & s.rhoc) & 1;
+    uint64_t Tu[U];
+    int pu[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const uint64_t cu = (uint64_t)u << tl;
+        Tu[u] = xor_cols(tks, cu);
+        pu[u] = __popcll(cu & s.rhoc) & 1;
+    }
+    // M row of the written branch (write pass)
+    const double m0r = bv ? s.Mr[1][0] : s.Mr[0][0], m0i = bv ? s.Mi[1][0] : s.Mi[0][0];
+    const double m1r = bv ? s.Mr[1][1] : s.Mr[0][1], m1i = bv ? s.Mi[1][1] : s.Mi[0][1];
+
+    double a0 = 0, a1 = 0;
+    const bool act = (unsigned int)tid < (1u << tl);   // blocks of < 32 cosets keep a full warp; the rest idle
+    for (unsigned int ch = act ? blockIdx.x : cx.nchunks; ch < cx.nchunks; ch += gridDim.x) {
+        const uint64_t cb = (uint64_t)ch << cx.chunk_log2;
+        const uint64_t bh = xor_cols(tks, cb) ^ Tt;
+        const int ph = (__popcll(cb & s.rhoc) & 1) ^ pt;
+        double vr[U][NTQ], vi[U][NTQ];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t b = bh ^ Tu[u];
+#pragma unroll
+            for (int i = 0; i < NTQ; i++) load_entry(mem + (b ^ s.tq[i]), vr[u][i], vi[u][i]);
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int pc = ph ^ pu[u];
+            // S[x][tau]
+            double s00r = 0, s00i = 0, s01r = 0, s01i = 0, s10r = 0, s10i = 0, s11r = 0, s11i = 0;
+#pragma unroll
+            for (int i = 0; i < NTQ; i++) {
+                const double xr = vr[u][i], xi = vi[u][i];
+                if (MOUT == 1 || s.tau0[i] == 0) { s00r += xr; s00i += xi; }
+                else { s01r += xr; s01i += xi; }
+                const bool neg = (pc ^ s.par[i]) != 0;
+                const double yr = neg ? -xr : xr, yi = neg ? -xi : xi;
+                if (MOUT == 1 || s.tau1[i] == 0) { s10r += yr; s10i += yi; }
+                else { s11r += yr; s11i += yi; }
+            }
+            const uint64_t b = bh ^ Tu[u];
+            if (WRITE) {
+                double o0r = m0r * s00r - m0i * s00i + m1r * s10r - m1i * s10i;
+                double o0i = m0r * s00i + m0i * s00r + m1r * s10i + m1i * s10r;
+                o0r *= sc;
+                o0i *= sc;
+                store_entry(mem + b, o0r, o0i);
+                a0 += o0r * o0r + o0i * o0i;
+                if (MOUT == 2) {
+                    double o1r = m0r * s01r - m0i * s01i + m1r * s11r - m1i * s11i;
+                    double o1i = m0r * s01i + m0i * s01r + m1r * s11i + m1i * s11r;
+                    o1r *= sc;
+                    o1i *= sc;
+                    store_entry(mem + (b ^ s.g), o1r, o1i);
+                    a0 += o1r * o1r + o1i * o1i;
+                }
+            } else {
+#pragma unroll
+                for (int bb = 0; bb < 2; bb++) {
+                    const double p0r = s.Mr[bb][0], p0i = s.Mi[bb][0], p1r = s.Mr[bb][1], p1i = s.Mi[bb][1];
+                    const double o0r = p0r * s00r - p0i * s00i + p1r * s10r - p1i * s10i;
+                    const double o0i = p0r * s00i + p0i * s00r + p1r * s10i + p1i * s10r;
+                    double nn = o0r * o0r + o0i * o0i;
+                    if (MOUT == 2) {
+                        const double o1r = p0r * s01r - p0i * s01i + p1r * s11r - p1i * s11i;
+                        const double o1i = p0r * s01i + p0i * s01r + p1r * s11i + p1i * s11r;
+                        nn += o1r * o1r + o1i * o1i;
+                    }
+                    if (bb == 0) a0 += nn;
+                    else a1 += nn;
+                }
+            }
+        }
+    }
+    double t0, t1;
+    if (!grid_reduce2(a0, a1, cx, t0, t1)) return;
+    if (WRITE) write_epilogue(cx, s.k, bv, t0);
+    else norm_epilogue(cx, s.k, t0, t1);
+}
+
+// Start of a string / sample: the unit table and a fresh state.
+template <typename E>
+__global__ void k_begin(E *mem, DevState *st) {
+    store_entry(mem, 1.0, 0.0);
+    st->prev = 1.0;
+    st->lsc = 0;
+    st->logscale = 0;
+    st->logp = 0;
+    st->sc = 1.0;
+    st->ek = 0;
+    st->bv = 0;
+    st->dead = 0;
+    st->counter = 0;
+    st->aux = 0;
+}
+
+// End of a string / sample: final log2 Pr, next item.
+__global__ void k_finish(DevState *st, double *logp_out, double *aux_out, int driver, int ns) {
+    const int it = st->item;
+    double lp;
+    if (driver == DRV_CHAIN1) lp = st->dead ? -INFINITY : log2(st->prev) + 2.0 * st->lsc - ns;
+    else lp = st->logp;
+    logp_out[it] = lp;
+    if (aux_out) aux_out[it] = driver == DRV_HYBRID ? st->logscale : st->aux;
+    st->item = it + 1;
+}
+
+__global__ void k_set_item(DevState *st, int item) { st->item = item; }
+
+// Live table at step K in logical (c, tq) order (the reference's prefix dump, gsamp2.cpp:170-174).
+template <typename E>
+__global__ void k_gather(const StepArgs s, const E *__restrict__ mem, int ntq, E *__restrict__ out) {
+    __shared__ uint64_t tks[40];
+    for (int j = threadIdx.x; j < 40; j += blockDim.x) tks[j] = s.tk[j];
+    __syncthreads();
+    const uint64_t N = (1ULL << s.nk) * (uint64_t)ntq;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t c = i / (uint64_t)ntq;
+        const int j = (int)(i % (uint64_t)ntq);
+        out[i] = mem[xor_cols(tks, c) ^ s.tq[j]];
+    }
+}
+
+// Resume: sum the slice dumps into the arena (gsamp2.cpp:196-205): entry (c, ti) of the sum is
+// sum_s f_s * dump_s[(c ^ cshift_s) * ntq + tperm_s[ti]], rounded to the arena type; the norm of the unrounded sum
+// goes to the state (prev), with logscale = L and aux = log2 Pr(prefix) = -K + log2(norm) + 2L.
+struct ResumeArgs {
+    const void *const *dumps;   // device array of nsl device pointers
+    const double *f;            // [nsl]
+    const uint64_t *cshift;     // [nsl]
+    const int *tperm;           // [nsl][4]
+    int nsl, ntq, K;
+    double L;
+};
+
+template <typename E>
+__global__ void k_resume_sum(const StepArgs s, E *__restrict__ mem, const ResumeArgs ra, const Ctx cx) {
+    __shared__ uint64_t tks[40];
+    for (int j = threadIdx.x; j < 40; j += blockDim.x) tks[j] = s.tk[j];
+    __syncthreads();
+    const uint64_t N = 1ULL << s.nk;
+    const int nt = ra.ntq;
+    double a0 = 0;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = xor_cols(tks, c);
+        for (int ti = 0; ti < nt; ti++) {
+            double ar = 0, ai = 0;
+            for (int sl = 0; sl < ra.nsl; sl++) {
+                const E *d = (const E *)ra.dumps[sl];
+                const uint64_t idx = (c ^ ra.cshift[sl]) * (uint64_t)nt + (uint64_t)ra.tperm[4 * sl + ti];
+                double vr, vi;
+                load_entry(d + idx, vr, vi);
+                ar += vr * ra.f[sl];
+                ai += vi * ra.f[sl];
+            }
+            store_entry(mem + (base ^ s.tq[ti]), ar, ai);
+            a0 += ar * ar + ai * ai;
+        }
+    }
+    double t0, t1;
+    if (!grid_reduce2(a0, 0.0, cx, t0, t1)) return;
+    DevState *st = cx.st;
+    st->prev = t0;
+    st->logscale = ra.L;
+    st->logp = 0;
+    st->dead = 0;
+    st->aux = -ra.K + log2(t0) + 2 * ra.L;
+}
+
+}  // namespace gsb

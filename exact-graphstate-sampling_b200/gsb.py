@@ -1,0 +1,305 @@
+"""Python binding (ctypes) of libgsb, the B200 executor of the in-place cut-rank DP (C ABI: include/gsb.h).
+
+Each method is one mode of the reference's executor command line (gsamp2.cpp:149-225): ``prob``, ``chain``,
+``sample`` (``sample`` / ``sample2`` seeding), ``hybrid``, ``prefix`` and ``resume``.  Strings are in STEP order
+(element k is the bit of the vertex processed at step k), given as str ('0', '1', '?') or int arrays (0, 1, -1).
+
+The library must be built (``python build.py``); there is no fallback: importing this module without
+libgsb.so, or opening an engine without a CUDA device, raises.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgsb.so")
+
+GSB_C64, GSB_C128 = 64, 128
+SEED_INT, SEED_SEQ = 0, 1
+
+ERROR_NAMES = {1: "usage", 2: "plan header", 3: "plan step", 4: "plan Tkeep", 5: "plan term", 6: "plan M",
+               7: "plan range", 8: "'?' before K", 9: "dump missing", 10: "bad dump", 11: "allocation",
+               12: "twist missing", 13: "twist line", 14: "twist range", 15: "plan layout", 20: "CUDA", 21: "state"}
+
+
+class GsbError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"gsb error {code} ({ERROR_NAMES.get(code, '?')}): {msg}")
+        self.code = code
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is not built; run build.py (the executor has no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    c = ctypes
+    P = c.c_void_p
+    i8p, dp, u64p = c.POINTER(c.c_int8), c.POINTER(c.c_double), c.POINTER(c.c_uint64)
+    sig = {
+        "gsb_version": (c.c_char_p, []),
+        "gsb_last_error": (c.c_char_p, []),
+        "gsb_open_file": (c.c_int, [c.c_char_p, c.c_int, c.c_int, c.POINTER(P)]),
+        "gsb_open_text": (c.c_int, [c.c_char_p, c.c_size_t, c.c_int, c.c_int, c.POINTER(P)]),
+        "gsb_close": (c.c_int, [P]),
+        "gsb_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+        "gsb_step_vertices": (c.c_int, [P, c.POINTER(c.c_int)]),
+        "gsb_prob": (c.c_int, [P, i8p, c.c_int64, dp]),
+        "gsb_chain": (c.c_int, [P, i8p, c.c_int64, dp, dp]),
+        "gsb_sample": (c.c_int, [P, c.c_int, c.c_uint64, c.c_int64, c.c_int64, i8p, dp]),
+        "gsb_sample_uniform": (c.c_int, [P, dp, c.c_int64, i8p, dp]),
+        "gsb_hybrid": (c.c_int, [P, i8p, c.c_int64, c.c_uint64, c.c_int64, i8p, dp, dp]),
+        "gsb_dump_shape": (c.c_int, [P, c.c_int, c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+        "gsb_prefix": (c.c_int, [P, i8p, c.c_int, P, dp, dp]),
+        "gsb_resume": (c.c_int, [P, i8p, c.c_int, c.c_uint64, c.c_int64, c.c_int, c.POINTER(P), dp, u64p, u64p,
+                                 i8p, dp, dp, dp]),
+        "gsb_chain_device": (c.c_int, [P, P, c.c_int64, P, P]),
+        "gsb_sample_device": (c.c_int, [P, P, c.c_int64, P, P]),
+        "gsb_synchronize": (c.c_int, [P]),
+        "gsb_set_stream": (c.c_int, [P, P]),
+        "gsb_profile_steps": (c.c_int, [P, i8p, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
+        "gsb_launches_per_item": (c.c_int, [P, c.c_int, c.POINTER(c.c_int64)]),
+        "gsb_validate_text": (c.c_int, [c.c_char_p, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
+                                        c.POINTER(c.c_int)]),
+        "gsb_cut_profile": (c.c_int, [c.c_int, c.POINTER(c.c_uint8), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+        "gsb_order_search": (c.c_int, [c.c_int, c.POINTER(c.c_uint8), c.c_uint64, c.c_int, c.c_int64,
+                                       c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = _load()
+EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
+           "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
+           "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
+           "gsb_synchronize", "gsb_set_stream", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_cut_profile", "gsb_order_search")
+
+
+def lib():
+    return _lib
+
+
+def _check(rc):
+    if rc:
+        raise GsbError(rc, _lib.gsb_last_error().decode(errors="replace"))
+
+
+def _ptr(a, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+def as_bits(strings, ns, allow_free=False):
+    """list of str / 2-D array -> contiguous int8 array [nstr][ns] with 0, 1 (and -1 for '?')."""
+    if isinstance(strings, np.ndarray):
+        a = np.ascontiguousarray(strings, dtype=np.int8)
+        if a.ndim == 1:
+            a = a[None, :]
+    else:
+        rows = []
+        for s in strings:
+            if isinstance(s, str):
+                s = s.strip()
+                rows.append([-1 if ch == "?" else int(ch) for ch in s])
+            else:
+                rows.append([int(x) for x in s])
+        a = np.array(rows, dtype=np.int8).reshape(len(rows), -1) if rows else np.zeros((0, ns), np.int8)
+    if a.shape[1] != ns:
+        raise ValueError(f"strings must have {ns} step bits, got {a.shape[1]}")
+    if not allow_free and (a < 0).any():
+        raise ValueError("'?' is only allowed in hybrid / resume strings")
+    return a
+
+
+class Engine:
+    """One plan on one GPU at one precision (64 = complex64 arena, 128 = complex128 arena)."""
+
+    def __init__(self, plan_path=None, precision=GSB_C64, device=0, text=None):
+        h = ctypes.c_void_p()
+        if text is not None:
+            b = text.encode() if isinstance(text, str) else bytes(text)
+            _check(_lib.gsb_open_text(b, len(b), int(precision), int(device), ctypes.byref(h)))
+        else:
+            _check(_lib.gsb_open_file(os.fsencode(plan_path), int(precision), int(device), ctypes.byref(h)))
+        self._h = h
+        n, ns, R, p = (ctypes.c_int() for _ in range(4))
+        _check(_lib.gsb_info(h, ctypes.byref(n), ctypes.byref(ns), ctypes.byref(R), ctypes.byref(p)))
+        self.n, self.ns, self.R, self.precision = n.value, ns.value, R.value, p.value
+        sv = np.zeros(max(self.ns, 1), np.int32)
+        _check(_lib.gsb_step_vertices(h, _ptr(sv, ctypes.c_int)))
+        self.step_vertices = [int(v) for v in sv[:self.ns]]
+        self.entry_dtype = np.complex128 if self.precision == 128 else np.complex64
+
+    @classmethod
+    def from_text(cls, text, precision=GSB_C64, device=0):
+        return cls(precision=precision, device=device, text=text)
+
+    @property
+    def handle(self):
+        if self._h is None:
+            raise GsbError(21, "engine is closed")
+        return self._h
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.gsb_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # --- modes ---
+    def prob(self, strings):
+        """'prob': log2 Pr of each string (two passes per step)."""
+        b = as_bits(strings, self.ns)
+        out = np.zeros(len(b), np.float64)
+        if len(b):
+            _check(_lib.gsb_prob(self.handle, _ptr(b, ctypes.c_int8), len(b), _ptr(out, ctypes.c_double)))
+        return out
+
+    def chain(self, strings):
+        """'chain': (log2 Pr [nstr], conditionals [nstr][ns]) with one pass per step."""
+        b = as_bits(strings, self.ns)
+        lp = np.zeros(len(b), np.float64)
+        cond = np.zeros((len(b), max(self.ns, 1)), np.float64)
+        if len(b):
+            _check(_lib.gsb_chain(self.handle, _ptr(b, ctypes.c_int8), len(b), _ptr(lp, ctypes.c_double),
+                                  _ptr(cond, ctypes.c_double)))
+        return lp, cond[:, :self.ns]
+
+    def sample(self, count, seed, first=0, seeding=SEED_INT):
+        """'sample' (seeding=SEED_INT) / 'sample2' (SEED_SEQ): (bits [count][ns], log2 Pr [count])."""
+        bits = np.zeros((count, max(self.ns, 1)), np.int8)
+        lp = np.zeros(count, np.float64)
+        if count:
+            _check(_lib.gsb_sample(self.handle, int(seeding), int(seed), int(first), int(count),
+                                   _ptr(bits, ctypes.c_int8), _ptr(lp, ctypes.c_double)))
+        return bits[:, :self.ns], lp
+
+    def sample_uniform(self, u):
+        """Chain-rule samples from caller uniforms u [count][ns]: bit k = u[k] < Pr(b_k = 1 | prefix)."""
+        u = np.ascontiguousarray(u, np.float64).reshape(-1, self.ns)
+        bits = np.zeros((len(u), max(self.ns, 1)), np.int8)
+        lp = np.zeros(len(u), np.float64)
+        if len(u):
+            _check(_lib.gsb_sample_uniform(self.handle, _ptr(u, ctypes.c_double), len(u), _ptr(bits, ctypes.c_int8),
+                                           _ptr(lp, ctypes.c_double)))
+        return bits[:, :self.ns], lp
+
+    def hybrid(self, strings, seed, first_line=0):
+        """'hybrid': '?' bits drawn from mt19937_64(seed + line); (bits, log2 Pr, conditionals)."""
+        f = as_bits(strings, self.ns, allow_free=True)
+        bits = np.zeros((len(f), max(self.ns, 1)), np.int8)
+        lp = np.zeros(len(f), np.float64)
+        cond = np.zeros((len(f), max(self.ns, 1)), np.float64)
+        if len(f):
+            _check(_lib.gsb_hybrid(self.handle, _ptr(f, ctypes.c_int8), len(f), int(seed), int(first_line),
+                                   _ptr(bits, ctypes.c_int8), _ptr(lp, ctypes.c_double), _ptr(cond, ctypes.c_double)))
+        return bits[:, :self.ns], lp, cond[:, :self.ns]
+
+    def dump_shape(self, K):
+        nk, ntq = ctypes.c_int(), ctypes.c_int()
+        _check(_lib.gsb_dump_shape(self.handle, int(K), ctypes.byref(nk), ctypes.byref(ntq)))
+        return nk.value, ntq.value
+
+    def prefix(self, string, K):
+        """'prefix': (dump [2^nk * ntq] of the arena dtype in (c, tq) order, logscale, log2 Pr(prefix))."""
+        f = as_bits([string], self.ns, allow_free=True)[0].copy()
+        nk, ntq = self.dump_shape(K)
+        dump = np.zeros((1 << nk) * ntq, self.entry_dtype)
+        ls, lp = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.gsb_prefix(self.handle, _ptr(f, ctypes.c_int8), int(K), dump.ctypes.data_as(ctypes.c_void_p),
+                               ctypes.byref(ls), ctypes.byref(lp)))
+        return dump, ls.value, lp.value
+
+    def resume(self, string, K, seed, line, dumps, logscales, twist=None):
+        """'resume': sum slice dumps, run steps K.. with '?' drawn; (bits, log2 Pr full, log2 Pr prefix, cond)."""
+        f = as_bits([string], self.ns, allow_free=True)[0].copy()
+        tabs = [np.ascontiguousarray(d, self.entry_dtype) for d in dumps]
+        ptrs = (ctypes.c_void_p * len(tabs))(*[t.ctypes.data for t in tabs])
+        ls = np.ascontiguousarray(logscales, np.float64)
+        cs = tq = None
+        if twist is not None:
+            cs = np.ascontiguousarray([t[0] for t in twist], np.uint64)
+            tq = np.ascontiguousarray([t[1] for t in twist], np.uint64)
+        bits = np.zeros(max(self.ns, 1), np.int8)
+        cond = np.zeros(max(self.ns, 1), np.float64)
+        lpf, lpp = ctypes.c_double(), ctypes.c_double()
+        _check(_lib.gsb_resume(self.handle, _ptr(f, ctypes.c_int8), int(K), int(seed), int(line), len(tabs), ptrs,
+                               _ptr(ls, ctypes.c_double), None if cs is None else _ptr(cs, ctypes.c_uint64),
+                               None if tq is None else _ptr(tq, ctypes.c_uint64), _ptr(bits, ctypes.c_int8),
+                               ctypes.byref(lpf), ctypes.byref(lpp), _ptr(cond, ctypes.c_double)))
+        return bits[:self.ns], lpf.value, lpp.value, cond[:self.ns]
+
+    # --- device-resident batches (torch tensors on this engine's GPU) ---
+    def chain_device(self, d_bits, d_log2p, d_cond=None):
+        _check(_lib.gsb_chain_device(self.handle, d_bits.data_ptr(), d_bits.shape[0], d_log2p.data_ptr(),
+                                     None if d_cond is None else d_cond.data_ptr()))
+
+    def sample_device(self, d_u, d_bits, d_log2p):
+        _check(_lib.gsb_sample_device(self.handle, d_u.data_ptr(), d_u.shape[0], d_bits.data_ptr(), d_log2p.data_ptr()))
+
+    def set_stream(self, cuda_stream):
+        """Queue work on a cudaStream_t (int handle, e.g. torch.cuda.current_stream().cuda_stream); 0 = own."""
+        _check(_lib.gsb_set_stream(self.handle, ctypes.c_void_p(int(cuda_stream) or None)))
+
+    def synchronize(self):
+        _check(_lib.gsb_synchronize(self.handle))
+
+    def profile_steps(self, string, mode=0):
+        """Per-step kernel times (ms) of one forced string: (write [ns], norm [ns]); mode 0 chain, 1 prob."""
+        f = as_bits([string], self.ns)[0].copy()
+        w = np.zeros(max(self.ns, 1), np.float32)
+        nrm = np.zeros(max(self.ns, 1), np.float32)
+        _check(_lib.gsb_profile_steps(self.handle, _ptr(f, ctypes.c_int8), int(mode), _ptr(w, ctypes.c_float),
+                                      _ptr(nrm, ctypes.c_float)))
+        return w[:self.ns], nrm[:self.ns]
+
+    def launches_per_item(self, mode):
+        n = ctypes.c_int64()
+        _check(_lib.gsb_launches_per_item(self.handle, int(mode), ctypes.byref(n)))
+        return n.value
+
+
+def validate_text(text):
+    """Parse + validate plan text on the host (no GPU): (n, nsteps, R); raises GsbError."""
+    b = text.encode() if isinstance(text, str) else bytes(text)
+    n, ns, R = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _check(_lib.gsb_validate_text(b, len(b), ctypes.byref(n), ctypes.byref(ns), ctypes.byref(R)))
+    return n.value, ns.value, R.value
+
+
+def cut_profile(A, order):
+    A = np.ascontiguousarray(np.asarray(A) & 1, np.uint8)
+    n = len(A)
+    o = np.ascontiguousarray(order, np.int32)
+    prof = np.zeros(max(n - 1, 1), np.int32)
+    _check(_lib.gsb_cut_profile(n, _ptr(A, ctypes.c_uint8), _ptr(o, ctypes.c_int), _ptr(prof, ctypes.c_int)))
+    return [int(x) for x in prof[:max(n - 1, 0)]]
+
+
+def order_search(A, seed=0, ngreedy=4, iters=20000):
+    A = np.ascontiguousarray(np.asarray(A) & 1, np.uint8)
+    n = len(A)
+    out = np.zeros(n, np.int32)
+    w = ctypes.c_int()
+    _check(_lib.gsb_order_search(n, _ptr(A, ctypes.c_uint8), int(seed), int(ngreedy), int(iters),
+                                 _ptr(out, ctypes.c_int), ctypes.byref(w)))
+    return [int(x) for x in out], w.value
+
+
+def version():
+    return _lib.gsb_version().decode()

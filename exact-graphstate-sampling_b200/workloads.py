@@ -1,0 +1,60 @@
+"""Benchmark workloads as plans: seeded circuit -> graph form -> order -> in-place plan text.
+
+``matching_n70_w30()`` is the headline instance: n = 70, 70 layers of CZ on seeded random perfect matchings with
+seeded random single-qubit Cliffords (seed 2), a Haar-random U3 per qubit, and the order the native search finds
+with seed 12, whose width is 30 (arena 2^30: 8.6 GB complex64, 17.2 GB complex128).
+"""
+import numpy as np
+
+import circuits
+import gsb
+from amp import Amplitudes
+from inplace import inplace_plan_text, plan_inplace, plan_width
+
+
+def build(n, body, tail, order):
+    am = Amplitudes(n, circuits.tableau_of(n, body), tail, order)
+    R = max(1, plan_width(am.steps))
+    st = plan_inplace(am.A, order, R)
+    return inplace_plan_text(st, R, am.M, n), st, R
+
+
+def matching_instance(n=70, depth=70, seed=2, order_seed=12, iters=60000):
+    n, body, tail = circuits.matching_circuit(n, depth, seed=seed)
+    from graphform import graph_form
+    A, _ = graph_form(circuits.tableau_of(n, body))
+    order, w = gsb.order_search(A, seed=order_seed, ngreedy=4, iters=iters)
+    text, st, R = build(n, body, tail, order)
+    return dict(name=f"matching_n{n}_d{depth}_s{seed}", n=n, body=body, tail=tail, order=order, width=R, plan=text,
+                steps=st)
+
+
+def matching_n70_w30():
+    return matching_instance(70, 70, 2, 12, 60000)
+
+
+def graph_state_instance(n=20, p=0.5, seed=1, order_seed=11, iters=20000):
+    n, body, tail = circuits.graph_state_circuit(n, p, seed=seed)
+    from graphform import graph_form
+    A, _ = graph_form(circuits.tableau_of(n, body))
+    order, w = gsb.order_search(A, seed=order_seed, ngreedy=4, iters=iters)
+    text, st, R = build(n, body, tail, order)
+    return dict(name=f"gnp_n{n}_s{seed}", n=n, body=body, tail=tail, order=order, width=R, plan=text, steps=st)
+
+
+def pass_bytes(steps, esize, passes="chain"):
+    """Algorithmic bytes of one string: a write pass moves E (2^{r_k} + 2^{r_{k+1}}), a norm pass E 2^{r_k}
+    (r_{k+1} = nk + log2 m).  passes: 'chain' (write only) or 'sample' (norm + write per step)."""
+    tot = 0
+    per = []
+    for s in steps:
+        r, rn = s["r"], s["rn"]
+        w = esize * ((1 << r) + (1 << rn))
+        nrm = esize * (1 << r) if passes == "sample" else 0
+        per.append((w, nrm))
+        tot += w + nrm
+    return tot, per
+
+
+def random_strings(ns, count, seed):
+    return np.random.default_rng(seed).integers(0, 2, size=(count, ns), dtype=np.int8)

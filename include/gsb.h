@@ -1,0 +1,140 @@
+/*
+ * gsb.h -- C ABI of the B200 executor for the in-place cut-rank dynamic program (libgsb.so).
+ *
+ * The reference has no in-process interface for this path: its seam is the executor process `gsamp2 <plan> <mode>`
+ * (gsamp2.cpp:1-6, 149-225), chosen by path through `doped_sampler.py --bin` (doped_sampler.py:28) and run by the
+ * cloud scripts and tests.  Each mode of that command line becomes one entry point here, with the same inputs
+ * (plan text, strings in step order, seeds, dump tables) and the same numbers out (bits, log2 Pr, conditionals,
+ * dump tables), so a ctypes / C / C++ caller can replace the subprocess call.  `gsb2` (the command line built on
+ * this library) keeps the reference's argv and stdout formats for callers that stay process based.
+ *
+ * Conventions
+ *   - Every function returns a status: 0 = GSB_OK, otherwise one of the codes below.  Codes 1-14 are the reference
+ *     executor's exit codes for the same failures.  Nothing calls exit(); gsb_last_error() gives a message
+ *     (thread-local, valid until the next call on this thread).
+ *   - Strings / bits are int8 arrays in STEP order (character k of a reference strings-file line is element k):
+ *     0, 1, or -1 for '?' where a mode allows it.  Multi-string arguments are row-major [nstr][nsteps].
+ *   - An engine owns one arena (2^R entries of complex64 or complex128) and one CUDA stream on one device.  Calls on
+ *     one engine must not overlap (one engine per host thread); different engines are independent.
+ *   - Host-buffer entry points are synchronous: they copy inputs in, run, and copy results out before returning.
+ */
+#ifndef GSB_H
+#define GSB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GSB_OK 0
+#define GSB_E_USAGE 1          /* bad argument (reference: exit 1, usage) */
+#define GSB_E_PLAN_HEADER 2    /* plan header "n nsteps R" unreadable (gsamp2.cpp:128) */
+#define GSB_E_PLAN_STEP 3      /* step line "v nk m g rhoc nterms" unreadable (gsamp2.cpp:131) */
+#define GSB_E_PLAN_TKEEP 4     /* Tkeep list unreadable (gsamp2.cpp:132) */
+#define GSB_E_PLAN_TERM 5      /* term "Tq x tau par" unreadable (gsamp2.cpp:133) */
+#define GSB_E_PLAN_M 6         /* M matrix unreadable (gsamp2.cpp:134) */
+#define GSB_E_PLAN_RANGE 7     /* nk > 40 or a term list outside what the plan format allows (gsamp2.cpp:135) */
+#define GSB_E_PREFIX_FREE 8    /* '?' before step K in prefix mode (gsamp2.cpp:168) */
+#define GSB_E_DUMP_MISSING 9   /* a dump table is missing (gsamp2.cpp:199) */
+#define GSB_E_DUMP_BAD 10      /* a dump table has the wrong shape (gsamp2.cpp:200) */
+#define GSB_E_ALLOC 11         /* arena allocation failed (gsamp2.cpp:142) */
+#define GSB_E_TWIST_MISSING 12 /* twist file missing (gsamp2.cpp:190) */
+#define GSB_E_TWIST_LINE 13    /* twist line unreadable (gsamp2.cpp:191) */
+#define GSB_E_TWIST_RANGE 14   /* twist shift outside the kept coordinates / coset offsets (gsamp2.cpp:192-194) */
+#define GSB_E_PLAN_LAYOUT 15   /* the plan breaks an in-place invariant (reference asserts inplace.py:85-88,131-137) */
+#define GSB_E_CUDA 20          /* CUDA runtime error (reference GPU port: exit 99, gsamp_cuda.cu:23) */
+#define GSB_E_STATE 21         /* invalid engine handle */
+
+#define GSB_C64 64             /* complex64 arena, FP64 arithmetic (the reference's default build) */
+#define GSB_C128 128           /* complex128 arena (the reference's -DGS_DOUBLE build, gsamp2.cpp:19-23) */
+
+#define GSB_SEED_INT 0         /* sample i uses std::mt19937_64(seed + i)                  ('sample', gsamp2.cpp:151) */
+#define GSB_SEED_SEQ 1         /* std::seed_seq{seed_lo, seed_hi, i_lo, i_hi, 0x9E3779B9}   ('sample2', gsamp2.cpp:159) */
+
+typedef struct gsb_engine gsb_engine;
+
+const char *gsb_version(void);
+const char *gsb_last_error(void);
+
+/* Load a plan (file path, or text in memory) and allocate the arena on `device`.
+ * Replaces the plan parse + arena set-up of gsamp2.cpp:128-147 / gsamp_cuda.cu:125-142.  The plan is also checked
+ * for the in-place invariants (independent addresses, writes inside the coset's own slots, addresses < 2^R). */
+int gsb_open_file(const char *plan_path, int precision, int device, gsb_engine **out);
+int gsb_open_text(const char *plan_text, size_t len, int precision, int device, gsb_engine **out);
+int gsb_close(gsb_engine *e);
+int gsb_info(const gsb_engine *e, int *n, int *nsteps, int *R, int *precision);
+/* qubit (vertex) of each step, nsteps entries */
+int gsb_step_vertices(const gsb_engine *e, int *out);
+
+/* 'prob': log2 Pr of each string, normalised two-pass chain (gsamp2.cpp:39-55, 217-223). */
+int gsb_prob(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p);
+
+/* 'chain': one pass per step; log2 Pr and every conditional Pr(b_k | b_1..b_{k-1}) (gsamp2.cpp:56-70, 217-222).
+ * cond is [nstr][nsteps]; may be NULL. */
+int gsb_chain(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p, double *cond);
+
+/* 'sample' / 'sample2': samples first .. first+count-1 of stream (seeding, seed): bits [count][nsteps] and log2 Pr
+ * (gsamp2.cpp:149-161).  The sample printed by the reference as "<bits> lp seed+i" is sample i here. */
+int gsb_sample(gsb_engine *e, int seeding, uint64_t seed, int64_t first, int64_t count, int8_t *bits, double *log2p);
+
+/* Exact chain-rule samples driven by caller-supplied uniforms u [count][nsteps] (bit k = u[k] < Pr(b_k = 1 | prefix)),
+ * the same draw rule as gsamp2.cpp:46-47. */
+int gsb_sample_uniform(gsb_engine *e, const double *u, int64_t count, int8_t *bits, double *log2p);
+
+/* 'hybrid': forced [nstr][nsteps] in {0,1,-1}; line i draws its '?' bits from std::mt19937_64(seed + first_line + i);
+ * bits, log2 Pr and all conditionals out (gsamp2.cpp:71-120, 209-216).  cond may be NULL. */
+int gsb_hybrid(gsb_engine *e, const int8_t *forced, int64_t nstr, uint64_t seed, int64_t first_line, int8_t *bits,
+               double *log2p, double *cond);
+
+/* Shape of the live table dumped at step K: 2^nk cosets x ntq offsets (gsamp2.cpp:121-125, 171). */
+int gsb_dump_shape(const gsb_engine *e, int K, int *nk, int *ntq);
+
+/* 'prefix': run the forced steps 0..K-1 of one string and copy out the live table in logical (c, tq) order, entries
+ * of the arena type (complex64 = 2 floats, complex128 = 2 doubles); *logscale and log2 Pr(prefix) as the reference
+ * prints them (gsamp2.cpp:162-175). */
+int gsb_prefix(gsb_engine *e, const int8_t *forced, int K, void *dump, double *logscale, double *log2p_prefix);
+
+/* 'resume': sum nslices dump tables (scaled by 2^(logscale_s - max)), read through the optional twist translation
+ * (cshift, tqshift per slice; both NULL for none), then run steps K..nsteps-1 drawing '?' bits from
+ * std::mt19937_64(seed + line) (gsamp2.cpp:176-208).  bits are full-length (forced prefix copied); cond [nsteps],
+ * entries K.. are written.  Dump entries are of the arena type. */
+int gsb_resume(gsb_engine *e, const int8_t *forced, int K, uint64_t seed, int64_t line, int nslices,
+               const void *const *dumps, const double *logscales, const uint64_t *cshift, const uint64_t *tqshift,
+               int8_t *bits, double *log2p_full, double *log2p_prefix, double *cond);
+
+/* Device-resident batches: all pointers are device memory on the engine's GPU.  Work is queued on the engine's
+ * stream; call gsb_synchronize before reading results. */
+int gsb_chain_device(gsb_engine *e, const int8_t *d_bits, int64_t nstr, double *d_log2p, double *d_cond);
+int gsb_sample_device(gsb_engine *e, const double *d_u, int64_t count, int8_t *d_bits, double *d_log2p);
+int gsb_synchronize(gsb_engine *e);
+/* Queue the engine's work on `cuda_stream` (a cudaStream_t of the engine's device; NULL = the engine's own stream),
+ * e.g. a framework's current stream, so events recorded there bracket the engine's kernels. */
+int gsb_set_stream(gsb_engine *e, void *cuda_stream);
+
+/* Per-step kernel timing for one forced string: ms_write[k] and ms_norm[k] (0 when a pass does not run) from CUDA
+ * events on the engine's stream, mode 0 = 'chain' (one pass per step), 1 = 'prob' (norm + write per step). */
+int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_write, float *ms_norm);
+
+/* Number of kernel launches one string / sample makes in the given mode (0 chain, 1 prob/sample, 2 hybrid). */
+int gsb_launches_per_item(const gsb_engine *e, int mode, int64_t *launches);
+
+/* ---- host-side helpers (no GPU needed) ---- */
+
+/* Parse and validate a plan without allocating anything on a device: the same checks gsb_open_* makes
+ * (reference parse gsamp2.cpp:128-139; layout invariants inplace.py:85-88, 131-137). */
+int gsb_validate_text(const char *plan_text, size_t len, int *n, int *nsteps, int *R);
+
+/* Cut-rank profile of a linear order of the graph A (n x n 0/1, row-major, n <= 128): prof[k-1] = rank over GF(2) of
+ * A[order[0..k-1], order[k..n-1]] for k = 1..n-1 (reference order.py:14-20). */
+int gsb_cut_profile(int n, const uint8_t *A, const int *order, int *prof);
+
+/* Heuristic order search (randomised greedy + local search on the key (max cut rank, steps at the max, log2 sum
+ * 2^r), as the reference's order2.py:16-28 / frontier_instance.py:29-37): best order found and its width. */
+int gsb_order_search(int n, const uint8_t *A, uint64_t seed, int ngreedy, int64_t iters, int *order_out, int *width_out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

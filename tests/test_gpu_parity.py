@@ -1,0 +1,261 @@
+"""Parity of the CUDA executor (through the C ABI) with the oracle and the reference's golden vectors.
+
+Tolerances: complex128 arena |d log2 Pr| <= 1e-9 and |d Pr| <= 1e-10 against the reference's complex128 build;
+complex64 arena |d log2 Pr| <= 1e-5 (the target the complex64 form is held to), conditionals <= 1e-6.
+Sampled bits must be identical to the reference's (same mt19937_64 streams); a bit could legitimately differ only
+when a uniform falls within rounding of its conditional, which none of these fixtures do.
+Negative controls (as in the reference's tests): a plan with the M rows swapped must disagree.
+"""
+import itertools
+import json
+import math
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import case_plan_text, parse_ref_lines
+
+pytestmark = pytest.mark.gpu
+
+TOL_LP = {128: 1e-9, 64: 1e-5}
+TOL_P = {128: 1e-10, 64: 1e-6}
+TOL_COND = {128: 1e-9, 64: 1e-6}
+
+
+def engine_from_text(text, prec):
+    import gsb
+    return gsb.Engine.from_text(text, precision=prec)
+
+
+def close_lp(a, b, tol, ptol=1e-10):
+    """log2 Pr values agree: both -inf, within tol, or (for tiny probabilities, where log2 amplifies absolute
+    rounding) within ptol as probabilities."""
+    if math.isinf(a) and math.isinf(b):
+        return True
+    if abs(a - b) <= tol:
+        return True
+    return max(a, b) < -20 and abs(2.0 ** a - 2.0 ** b) <= ptol
+
+
+@pytest.mark.parametrize("prec", [128, 64])
+def test_small_prob_chain_vs_reference(executor_cases, planner_cases, prec):
+    texts = {c["name"]: c["inplace_plan"] for c in planner_cases["cases"]}
+    worst_lp = worst_c = 0.0
+    for ec in executor_cases:
+        with engine_from_text(texts[ec["name"]], prec) as eng:
+            lp = eng.prob(ec["strings"])
+            ref = np.array([float(x) for x in ec[f"prob{prec}"]])
+            p, pr = np.exp2(lp), np.exp2(ref)
+            assert np.abs(p - pr).max() <= TOL_P[prec]
+            fin = pr > 1e-12
+            worst_lp = max(worst_lp, np.abs(lp[fin] - ref[fin]).max(initial=0))
+            lpc, cond = eng.chain(ec["strings"])
+            refc = parse_ref_lines(ec[f"chain{prec}"])
+            for i, row in enumerate(refc):
+                assert close_lp(lpc[i], float(row[0]), TOL_LP[prec], TOL_P[prec])
+                rc = np.array([float(x) for x in row[1:]])
+                worst_c = max(worst_c, np.abs(cond[i] - rc).max())
+    assert worst_lp <= TOL_LP[prec], worst_lp
+    assert worst_c <= max(TOL_COND[prec], 1e-9 if prec == 128 else 1e-6), worst_c
+
+
+@pytest.mark.parametrize("prec", [128, 64])
+def test_small_samples_bit_exact(executor_cases, planner_cases, prec):
+    import gsb
+    texts = {c["name"]: c["inplace_plan"] for c in planner_cases["cases"]}
+    for ec in executor_cases:
+        with engine_from_text(texts[ec["name"]], prec) as eng:
+            for key, seeding, seed in ((f"sample{prec}", gsb.SEED_INT, 1000), (f"sample2_{prec}", gsb.SEED_SEQ, 5)):
+                ref = parse_ref_lines(ec[key])
+                bits, lp = eng.sample(len(ref), seed, seeding=seeding)
+                for i, row in enumerate(ref):
+                    assert "".join(str(int(b)) for b in bits[i]) == row[0], (ec["name"], key, i)
+                    assert close_lp(lp[i], float(row[1]), TOL_LP[prec])
+                    assert int(row[2]) == seed + i
+
+
+@pytest.mark.parametrize("prec", [128, 64])
+def test_small_hybrid(executor_cases, planner_cases, prec):
+    texts = {c["name"]: c["inplace_plan"] for c in planner_cases["cases"]}
+    for ec in executor_cases:
+        with engine_from_text(texts[ec["name"]], prec) as eng:
+            bits, lp, cond = eng.hybrid(ec["hybrid_lines"], 9)
+            for i, row in enumerate(parse_ref_lines(ec[f"hybrid{prec}"])):
+                assert "".join(str(int(b)) for b in bits[i]) == row[0]
+                assert close_lp(lp[i], float(row[1]), TOL_LP[prec])
+                assert np.abs(cond[i] - np.array([float(x) for x in row[2:]])).max() <= TOL_COND[prec]
+
+
+@pytest.mark.parametrize("prec", [128, 64])
+def test_small_prefix_resume(executor_cases, planner_cases, prec):
+    """prefix dumps + resume (one slice) against the reference's printed lines and the oracle's dump tables."""
+    from oracle import Oracle
+    texts = {c["name"]: c["inplace_plan"] for c in planner_cases["cases"]}
+    with tempfile.TemporaryDirectory() as td:
+        for ec in executor_cases:
+            K = ec["K"]
+            path = os.path.join(td, "p.txt")
+            open(path, "w").write(texts[ec["name"]])
+            orc = Oracle(path, prec)
+            pre_ref = parse_ref_lines(ec[f"prefix{prec}"])
+            res_ref = parse_ref_lines(ec[f"resume{prec}"])
+            with engine_from_text(texts[ec["name"]], prec) as eng:
+                for li, line in enumerate(ec["prefix_lines"]):
+                    dump, ls, lp = eng.prefix(line, K)
+                    odump, ols, olp = orc.prefix(line, K)
+                    assert close_lp(lp, float(pre_ref[li][1]), TOL_LP[prec])
+                    assert abs(ls - float(pre_ref[li][2])) <= 1e-6
+                    assert abs(ls - ols) <= 1e-9
+                    assert np.abs(dump.astype(np.complex128) - odump).max() <= (1e-12 if prec == 128 else 1e-6)
+                    bits, lpf, lpp, cond = eng.resume(line, K, 3, li, [dump], [ls])
+                    row = res_ref[li]
+                    assert "".join(str(int(b)) for b in bits) == row[0]
+                    assert close_lp(lpf, float(row[1]), TOL_LP[prec])
+                    assert close_lp(lpp, float(row[2]), TOL_LP[prec])
+                    rc = np.array([float(x) for x in row[3:]])
+                    assert np.abs(cond[K:] - rc).max() <= TOL_COND[prec]
+            orc.close()
+
+
+def test_statevector_every_string(planner_cases):
+    """End to end through this repository's planner: Born probabilities of every string against a dense
+    statevector (complex128 <= 1e-10, complex64 <= 1e-6); negative control with M rows swapped."""
+    from oracle import statevector
+    from inplace import inplace_plan_text
+    worst = {128: 0.0, 64: 0.0}
+    ctrl = 0.0
+    for case in planner_cases["cases"]:
+        n = case["n"]
+        if n > 10:
+            continue
+        text, am, st, R = case_plan_text(case)
+        psi2 = statevector.probabilities(n, [tuple(x) for x in case["body"]] + [tuple(x) for x in case["tail"]])
+        strings, idx = [], []
+        for bits in itertools.product((0, 1), repeat=n):
+            strings.append([bits[s["v"]] for s in st])
+            idx.append(statevector.index_of(bits))
+        for prec in (128, 64):
+            with engine_from_text(text, prec) as eng:
+                p = np.exp2(eng.prob(np.array(strings, np.int8)))
+                worst[prec] = max(worst[prec], np.abs(p - psi2[idx]).max())
+        if any(s["m"] == 2 for s in st) and ctrl < 1e-2:
+            bad = inplace_plan_text(st, R, [m[::-1].copy() for m in am.M], n)
+            with engine_from_text(bad, 128) as eng:
+                p = np.exp2(eng.prob(np.array(strings, np.int8)))
+                ctrl = max(ctrl, np.abs(p - psi2[idx]).max())
+    assert worst[128] <= 1e-10 and worst[64] <= 1e-6, worst
+    assert ctrl > 1e-2
+
+
+def test_zero_probability_branches():
+    """A circuit whose tail is Clifford has zero-probability strings: log2 Pr = -inf and conditionals 0 after the
+    first impossible step, as the reference prints them (gsamp2.cpp:48,67)."""
+    from amp import Amplitudes
+    from circuits import tableau_of
+    from inplace import inplace_plan_text, plan_inplace
+    from oracle import Oracle
+    n = 4
+    body = [("h", [0]), ("cz", [0, 1]), ("h", [2]), ("cz", [2, 3]), ("cz", [1, 2])]
+    tail = [("h", [q]) for q in range(n)]
+    am = Amplitudes(n, tableau_of(n, body), tail, [0, 1, 2, 3])
+    R = max(1, max(max(s["r"], s["rn"]) for s in am.steps))
+    st = plan_inplace(am.A, [0, 1, 2, 3], R)
+    text = inplace_plan_text(st, R, am.M, n)
+    strings = [list(b) for b in itertools.product((0, 1), repeat=n)]
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "p.txt")
+        open(path, "w").write(text)
+        orc = Oracle(path, 128)
+        with engine_from_text(text, 128) as eng:
+            lp = eng.prob(strings)
+            lpc, cond = eng.chain(strings)
+        ninf = 0
+        for i, s in enumerate(strings):
+            o = orc.prob(s)
+            oc, ocond = orc.chain1(s)
+            if math.isinf(o):
+                ninf += 1
+                assert math.isinf(lp[i]) and math.isinf(lpc[i])
+            else:
+                assert abs(lp[i] - o) < 1e-9 and abs(lpc[i] - oc) < 1e-9
+            assert np.abs(cond[i] - ocond).max() < 1e-12
+        assert ninf > 0
+
+
+# ---------------------------------------------------------------- the pinned width-30 instance
+
+def _lines(path):
+    return [ln.rstrip("\n") for ln in open(path) if ln.strip()]
+
+
+@pytest.fixture(scope="module")
+def w30_engines(w30_dir):
+    import gsb
+    engs = {p: gsb.Engine(os.path.join(w30_dir, "nq70_inplace_plan.txt"), precision=p) for p in (64, 128)}
+    yield engs
+    for e in engs.values():
+        e.close()
+
+
+def test_w30_gate_kat(w30_engines, w30_dir):
+    """cloud_ibmxeb/run.sh:19-21: two log2 Pr within 1e-5, in both precisions, prob and chain modes."""
+    gate = json.load(open(os.path.join(w30_dir, "gate_log2p.json")))
+    strings = _lines(os.path.join(w30_dir, "gate_strings.txt"))
+    for prec, eng in w30_engines.items():
+        lp = eng.prob(strings)
+        lpc, _ = eng.chain(strings)
+        for a, b, g in zip(lp, lpc, gate["log2p"]):
+            assert abs(a - g) <= gate["tol"] and abs(b - g) <= gate["tol"], (prec, a, b, g)
+    ref_path = os.path.join(w30_dir, "gate_ref_outputs.json")
+    if os.path.exists(ref_path):
+        ref = json.load(open(ref_path))
+        for prec, eng in w30_engines.items():
+            lp = eng.prob(strings)
+            r = [float(x) for x in ref[f"prob{prec}"]]
+            assert np.abs(lp - r).max() <= (1e-8 if prec == 128 else 2e-6)
+            lpc, cond = eng.chain(strings)
+            for i, row in enumerate(ref[f"chain{prec}"]):
+                v = [float(x) for x in row.split()]
+                assert abs(lpc[i] - v[0]) <= (1e-8 if prec == 128 else 2e-6)
+                assert np.abs(cond[i] - np.array(v[1:])).max() <= (1e-9 if prec == 128 else 1e-6)
+
+
+def test_w30_ibm_shots(w30_engines, w30_dir):
+    """First 64 of the 1,726 exact IBM-shot probabilities (results/ibmxeb/ibm_out.txt) and their chain
+    conditionals (results/chain/ibm_fwd_chain.txt)."""
+    strings = _lines(os.path.join(w30_dir, "ibm_strings_64.txt"))
+    ref = np.array([float(x) for x in _lines(os.path.join(w30_dir, "ibm_log2p_64.txt"))])
+    chain = [[float(x) for x in ln.split()] for ln in _lines(os.path.join(w30_dir, "ibm_chain_64.txt"))]
+    for prec, eng in w30_engines.items():
+        lp, cond = eng.chain(strings)
+        assert np.abs(lp - ref).max() <= 1e-5, prec
+        assert np.abs(lp - np.array([c[0] for c in chain])).max() <= 1e-5
+        assert np.abs(cond - np.array([c[1:] for c in chain])).max() <= 1e-6
+
+
+def test_w30_samples_bit_exact(w30_engines, w30_dir):
+    """results/laptop_samples_w30.txt ('sample', seeds 2000000+) and results/samples_nq70_reseeded.txt
+    ('sample2', seeds 3000000+): identical bits, log2 Pr within 1e-5."""
+    import gsb
+    for fname, seeding, seed in (("laptop_samples_w30.txt", gsb.SEED_INT, 2000000),
+                                 ("samples2_16.txt", gsb.SEED_SEQ, 3000000)):
+        ref = [ln.split() for ln in _lines(os.path.join(w30_dir, fname))]
+        for prec, eng in w30_engines.items():
+            bits, lp = eng.sample(len(ref), seed, seeding=seeding)
+            for i, row in enumerate(ref):
+                assert "".join(str(int(b)) for b in bits[i]) == row[0], (fname, prec, i)
+                assert abs(lp[i] - float(row[1])) <= 1e-5
+                assert int(row[2]) == seed + i
+
+
+def test_w30_regenerated_plan_same_probabilities(w30_engines, w30_dir):
+    """The plan this repository's planner writes for the #151 circuit (equal to the current reference planner's)
+    has another arena layout than the shipped plan but must give the same probabilities."""
+    import gsb
+    strings = _lines(os.path.join(w30_dir, "ibm_strings_64.txt"))[:8]
+    with gsb.Engine(os.path.join(w30_dir, "nq70_inplace_plan_regen.txt"), precision=128) as e2:
+        a = e2.chain(strings)[0]
+    b = w30_engines[128].chain(strings)[0]
+    assert np.abs(a - b).max() <= 1e-8
