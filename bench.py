@@ -51,7 +51,24 @@ def parse():
     ap.add_argument("--c128-amps", type=int, default=8)
     ap.add_argument("--c128-samples", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--arith", type=int, default=32, choices=[32, 64],
+                    help="arithmetic of the complex64 wide-step kernels (32: FP32; 64: exact sums + FP64 rotation)")
+    ap.add_argument("--profile-chain", type=int, default=0, metavar="N",
+                    help="only evaluate N strings in chain mode on --profile-workload (for ncu captures)")
+    ap.add_argument("--profile-workload", default="n70", choices=["n70", "n62"])
+    ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 128])
     return ap.parse_args()
+
+
+def profile_chain(args):
+    """A bare run for profilers: build the workload, evaluate N strings in chain mode, print nothing else."""
+    import gsb
+    import workloads
+    w = workloads.matching_n70_w30() if args.profile_workload == "n70" else workloads.matching_instance(62, 62, 3, 13)
+    with gsb.Engine.from_text(w["plan"], precision=args.profile_precision) as eng:
+        eng.set_arith(args.arith)
+        lp, _ = eng.chain(workloads.random_strings(len(w["steps"]), args.profile_chain, seed=9))
+    print(json.dumps({"workload": w["name"], "width": w["width"], "log2p": [float(x) for x in lp]}))
 
 
 def peaks():
@@ -204,7 +221,9 @@ def run_gsb(args):
     hbm_peak, peak_kind = peaks()
 
     eng = gsb.Engine.from_text(w["plan"], precision=64, device=local)
-    stream = torch.cuda.current_stream()
+    eng.set_arith(args.arith)
+    stream = torch.cuda.Stream()                  # a real stream: the engine's kernels and the events share it
+    torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
     strings = workloads.random_strings(ns, (W + K) * A, seed=1000 + rank)
     d_bits = torch.from_numpy(strings).to("cuda")
@@ -323,9 +342,9 @@ def run_gsb(args):
     out = {
         "metric": METRIC, "value": value, "unit": "amps/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c64 arena, f64 arithmetic", "data": "synthetic",
+        "dtype": f"c64 arena, f{args.arith} arithmetic", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": 70, "width": w["width"], "strings_per_step": A, "mode": "chain",
-                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
+                   "arith": args.arith, "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
         "s_per_sample": s_per_sample64, "samples_per_s": world / s_per_sample64,
         "c128": c128, "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
         "clocks": clk.summary(),
@@ -351,7 +370,9 @@ def run_gsb(args):
 
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.profile_chain:
+        profile_chain(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_gsb(a)

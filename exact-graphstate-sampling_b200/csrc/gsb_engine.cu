@@ -76,9 +76,33 @@ static void *pick_step_kernel(int ntq, int m, int U, bool write) {
     return pick_m<E, 1>(m, U, write);
 }
 
+// wide-step kernels: U = 4 coset groups per thread for 1-2 offsets, 2 for 4 offsets (register budget)
+template <int NTQ, int M>
+static void *pick_pair64(bool write, bool fp32) {
+    constexpr int U = NTQ == 4 ? 2 : 4;
+    if (fp32) return write ? (void *)k_pair64<float, NTQ, M, U, true> : (void *)k_pair64<float, NTQ, M, U, false>;
+    return write ? (void *)k_pair64<double, NTQ, M, U, true> : (void *)k_pair64<double, NTQ, M, U, false>;
+}
+template <int NTQ, int M>
+static void *pick_wide128(bool write) {
+    constexpr int U = NTQ == 4 ? 2 : 4;
+    return write ? (void *)k_wide128<NTQ, M, U, true> : (void *)k_wide128<NTQ, M, U, false>;
+}
+static void *pick_wide(int prec, int ntq, int m, bool write, bool fp32) {
+    if (prec == 64) {
+        if (ntq == 4) return m == 2 ? pick_pair64<4, 2>(write, fp32) : pick_pair64<4, 1>(write, fp32);
+        if (ntq == 2) return m == 2 ? pick_pair64<2, 2>(write, fp32) : pick_pair64<2, 1>(write, fp32);
+        return m == 2 ? pick_pair64<1, 2>(write, fp32) : pick_pair64<1, 1>(write, fp32);
+    }
+    if (ntq == 4) return m == 2 ? pick_wide128<4, 2>(write) : pick_wide128<4, 1>(write);
+    if (ntq == 2) return m == 2 ? pick_wide128<2, 2>(write) : pick_wide128<2, 1>(write);
+    return m == 2 ? pick_wide128<1, 2>(write) : pick_wide128<1, 1>(write);
+}
+
 struct Engine {
     HPlan plan;
     int prec = 64, dev = 0, sms = 0;
+    int arith = 32;                      // arithmetic of the complex64 wide-step kernels: 32 (FP32) or 64 (FP64)
     size_t esize = 8;
     void *mem = nullptr;
     cudaStream_t stream = nullptr;       // where work is queued (own_stream unless the caller set one)
@@ -127,6 +151,21 @@ struct Engine {
     Launch shape(const StepArgs &a, bool write) {
         Launch L;
         const uint64_t N = 1ULL << a.nk;
+        // wide steps: the pair kernel (complex64, needs coset bit 0 = arena bit 0) or the complex128 kernel
+        const int uw = a.ntq == 4 ? 2 : 4;
+        const bool wide64 = prec == 64 && a.nk >= 11 && a.tk[0] == 1;
+        const bool wide128 = prec == 128 && a.nk >= 10;
+        if (wide64 || wide128) {
+            L.block = 256;
+            L.U = uw;
+            L.tl = 8;
+            L.cl = (wide64 ? 9 : 8) + (uw == 4 ? 2 : 1);
+            L.nchunks = (unsigned int)(N >> L.cl);
+            L.fn = pick_wide(prec, a.ntq, a.m, write, arith == 32);
+            const int cap_blocks = occupancy(L.fn, L.block) * sms;
+            L.grid = (int)std::min<uint64_t>(L.nchunks, (uint64_t)cap_blocks);
+            return L;
+        }
         // blocks of at least one full warp (the reductions shuffle over 32 lanes); below 32 cosets the threads
         // tid >= 2^nk idle
         if (N >= 1024) { L.block = 256; L.U = 4; L.tl = 8; }
@@ -720,6 +759,23 @@ int gsb_synchronize(gsb_engine *e) {
     Engine *E = eng(e);
     DevGuard g(E->dev);
     GSB_CK(cudaStreamSynchronize(E->stream));
+    return 0;
+}
+
+int gsb_set_arith(gsb_engine *e, int bits) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (bits != 32 && bits != 64) return fail(GSB_E_USAGE, "arithmetic must be 32 or 64");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    if (bits == E->arith) return 0;
+    E->arith = bits;
+    for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);
+    E->graphs.clear();
+    for (int k = 0; k < E->plan.ns; k++) {
+        E->lw[(size_t)k] = E->shape(E->args[(size_t)k], true);
+        E->ln[(size_t)k] = E->shape(E->args[(size_t)k], false);
+    }
     return 0;
 }
 

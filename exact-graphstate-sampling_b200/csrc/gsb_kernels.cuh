@@ -325,6 +325,280 @@ __global__ void __launch_bounds__(256) k_step(const StepArgs s, E *__restrict__ 
     else norm_epilogue(cx, s.k, t0, t1);
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Wide-step kernels.  Steps with at least 2^11 cosets run one of these instead of k_step; both
+//   * walk their block's range of chunks in Gray-code order, so consecutive chunks differ in one coset bit and the
+//     chunk's base address is updated with one XOR (chunk i covers cosets gray(i) * 2^chunk_log2 + [0, 2^chunk_log2));
+//   * fold the step's scale into the M row of the write pass (one uniform multiply per kernel, not per entry);
+//   * prepare the write/norm decision exactly as k_step does (same prologue, same epilogues).
+
+struct Prologue {
+    int bv;
+    double sc;
+    bool skip;
+};
+
+__device__ __forceinline__ Prologue step_prologue(const StepArgs &s, const Ctx &cx, bool write) {
+    Prologue P{0, 1.0, false};
+    DevState *st = cx.st;
+    if (*(volatile int *)&st->dead) { P.skip = true; return P; }
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    if (write) {
+        if (cx.driver == DRV_HYBRID) {
+            const int f = cx.forced[row + s.k];
+            P.bv = f >= 0 ? f : st->bv;
+            P.sc = 1.0 / sqrt(st->prev);
+        } else if (cx.driver == DRV_CHAIN1) {
+            P.bv = cx.forced[row + s.k];
+            P.sc = st->sc;
+        } else {
+            P.bv = st->bv;
+            P.sc = st->sc;
+        }
+    } else if (cx.driver == DRV_HYBRID && cx.forced[row + s.k] >= 0) {
+        P.skip = true;
+    }
+    return P;
+}
+
+// chunk range of this block: [i0, i1) of gray-code indices
+__device__ __forceinline__ void block_range(unsigned int nch, unsigned int &i0, unsigned int &i1) {
+    const unsigned int per = (nch + gridDim.x - 1) / gridDim.x;
+    i0 = min(nch, blockIdx.x * per);
+    i1 = min(nch, i0 + per);
+}
+
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
+
+// complex64 arena, two adjacent cosets per thread and per 16-byte access.  Requires Tkeep[0] = 1 (coset bit 0 is arena
+// bit 0, as the planner lays out wide steps): cosets c (even) and c + 1 have bases b and b ^ 1, so each coset offset
+// tq, and the two write targets, address one aligned pair of entries; a swap flag (bit 0 of the address) says which
+// half belongs to the even coset.  Norms are accumulated in FP64.
+// Arithmetic type T:
+//   double: the coset's pair sums of float entries are exact in FP64 (the compensated form), the rotation by M is
+//           done in FP64, and the only rounding is the store to complex64 -- the arithmetic of the reference's
+//           complex64 build (gsamp2.cpp:32-38, 52);
+//   float : sums and rotation in FP32 (a few roundings per entry; faster on the FP32 pipe).
+// Chunk = 256 threads x U pairs = 2^(9 + log2 U) cosets; pair u of thread t covers cosets 2t + 512u + {0, 1}.
+template <typename T, int NTQ, int MOUT, int U, bool WRITE>
+__global__ void __launch_bounds__(256) k_pair64(const StepArgs s, float2 *__restrict__ mem, const Ctx cx) {
+    const Prologue P = step_prologue(s, cx, WRITE);
+    if (P.skip) return;
+    __shared__ uint64_t tks[40];
+    for (int j = threadIdx.x; j < 40; j += blockDim.x) tks[j] = s.tk[j];
+    __syncthreads();
+    const int tid = threadIdx.x;
+    const int cl = cx.chunk_log2;
+    float4 *__restrict__ mem4 = reinterpret_cast<float4 *>(mem);
+    // M rows: write pass uses sc * M[bv][x]; norm pass both rows
+    T wr[2][2], wi[2][2];
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+        for (int x = 0; x < 2; x++) {
+            const int bb = WRITE ? P.bv : b;
+            const double f = WRITE ? P.sc : 1.0;
+            wr[b][x] = (T)(f * s.Mr[bb][x]);
+            wi[b][x] = (T)(f * s.Mi[bb][x]);
+        }
+    uint64_t Tt = 0;
+    for (int j = 0; j < 8; j++)
+        if ((tid >> j) & 1) Tt ^= tks[j + 1];
+    const int pt = __popcll((uint64_t)(2 * tid) & s.rhoc) & 1;
+    uint64_t Tu[U];
+    int pu[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const uint64_t cu = (uint64_t)u << 9;
+        Tu[u] = xor_cols(tks, cu);
+        pu[u] = __popcll(cu & s.rhoc) & 1;
+    }
+    const int podd = (int)(s.rhoc & 1);
+    double a0 = 0, a1 = 0;
+    unsigned int i0, i1;
+    block_range(cx.nchunks, i0, i1);
+    uint64_t bh = 0;
+    int ph = 0;
+    if (i0 < i1) {
+        const uint64_t cb = (uint64_t)(i0 ^ (i0 >> 1)) << cl;
+        bh = xor_cols(tks, cb) ^ Tt;
+        ph = (__popcll(cb & s.rhoc) & 1) ^ pt;
+    }
+    for (unsigned int i = i0; i < i1; i++) {
+        if (i > i0) {
+            const int j = __ffs((int)i) - 1 + cl;   // gray(i) = gray(i - 1) ^ 2^ctz(i)
+            bh ^= tks[j];
+            ph ^= (int)((s.rhoc >> j) & 1);
+        }
+        float4 v[U][NTQ];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t be = bh ^ Tu[u];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) v[u][t] = mem4[(be ^ s.tq[t]) >> 1];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t be = bh ^ Tu[u];
+            const int pe = ph ^ pu[u];
+            T S[2][2][2][2] = {};   // [coset e/o][x][tau][re/im]
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                const bool sw = ((be ^ s.tq[t]) & 1) != 0;
+                const T er = sw ? v[u][t].z : v[u][t].x, ei = sw ? v[u][t].w : v[u][t].y;
+                const T orr = sw ? v[u][t].x : v[u][t].z, oi = sw ? v[u][t].y : v[u][t].w;
+                const int t0 = MOUT == 1 ? 0 : s.tau0[t], t1 = MOUT == 1 ? 0 : s.tau1[t];
+                const bool ne = ((pe ^ s.par[t]) & 1) != 0, no = ((pe ^ podd ^ s.par[t]) & 1) != 0;
+#pragma unroll
+                for (int tau = 0; tau < MOUT; tau++) {
+                    if (t0 == tau) {
+                        S[0][0][tau][0] += er; S[0][0][tau][1] += ei;
+                        S[1][0][tau][0] += orr; S[1][0][tau][1] += oi;
+                    }
+                    if (t1 == tau) {
+                        S[0][1][tau][0] += ne ? -er : er; S[0][1][tau][1] += ne ? -ei : ei;
+                        S[1][1][tau][0] += no ? -orr : orr; S[1][1][tau][1] += no ? -oi : oi;
+                    }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < (WRITE ? 1 : 2); b++) {
+                float o[2][MOUT][2];   // [eo][tau][re/im], rounded to the arena type
+                T nn = 0;
+#pragma unroll
+                for (int eo = 0; eo < 2; eo++)
+#pragma unroll
+                    for (int tau = 0; tau < MOUT; tau++) {
+                        const T *s0 = S[eo][0][tau], *s1 = S[eo][1][tau];
+                        T r = wr[b][0] * s0[0];
+                        r = fmaT(-wi[b][0], s0[1], r);
+                        r = fmaT(wr[b][1], s1[0], r);
+                        r = fmaT(-wi[b][1], s1[1], r);
+                        T im = wr[b][0] * s0[1];
+                        im = fmaT(wi[b][0], s0[0], im);
+                        im = fmaT(wr[b][1], s1[1], im);
+                        im = fmaT(wi[b][1], s1[0], im);
+                        o[eo][tau][0] = (float)r;
+                        o[eo][tau][1] = (float)im;
+                        nn = fmaT(r, r, nn);
+                        nn = fmaT(im, im, nn);
+                    }
+                if (b == 0) a0 += (double)nn;
+                else a1 += (double)nn;
+                if (WRITE) {
+                    const bool s0w = (be & 1) != 0;
+                    mem4[be >> 1] = s0w ? make_float4(o[1][0][0], o[1][0][1], o[0][0][0], o[0][0][1])
+                                        : make_float4(o[0][0][0], o[0][0][1], o[1][0][0], o[1][0][1]);
+                    if (MOUT == 2) {
+                        const uint64_t bg = be ^ s.g;
+                        const bool s1w = (bg & 1) != 0;
+                        const int t1 = MOUT - 1;
+                        mem4[bg >> 1] = s1w ? make_float4(o[1][t1][0], o[1][t1][1], o[0][t1][0], o[0][t1][1])
+                                            : make_float4(o[0][t1][0], o[0][t1][1], o[1][t1][0], o[1][t1][1]);
+                    }
+                }
+            }
+        }
+    }
+    double t0, t1;
+    if (!grid_reduce2(a0, a1, cx, t0, t1)) return;
+    if (WRITE) write_epilogue(cx, s.k, P.bv, t0);
+    else norm_epilogue(cx, s.k, t0, t1);
+}
+
+// complex128 arena, one coset per thread and per 16-byte entry; FP64 arithmetic.
+// Chunk = 256 threads x U cosets = 2^(8 + log2 U) cosets; coset u of thread t is t + 256u.
+template <int NTQ, int MOUT, int U, bool WRITE>
+__global__ void __launch_bounds__(256) k_wide128(const StepArgs s, double2 *__restrict__ mem, const Ctx cx) {
+    const Prologue P = step_prologue(s, cx, WRITE);
+    if (P.skip) return;
+    __shared__ uint64_t tks[40];
+    for (int j = threadIdx.x; j < 40; j += blockDim.x) tks[j] = s.tk[j];
+    __syncthreads();
+    const int tid = threadIdx.x;
+    const int cl = cx.chunk_log2;
+    double wr[2][2], wi[2][2];
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+        for (int x = 0; x < 2; x++) {
+            const int bb = WRITE ? P.bv : b;
+            const double f = WRITE ? P.sc : 1.0;
+            wr[b][x] = f * s.Mr[bb][x];
+            wi[b][x] = f * s.Mi[bb][x];
+        }
+    uint64_t Tt = 0;
+    for (int j = 0; j < 8; j++)
+        if ((tid >> j) & 1) Tt ^= tks[j];
+    const int pt = __popcll((uint64_t)tid & s.rhoc) & 1;
+    uint64_t Tu[U];
+    int pu[U];
+#pragma unroll
+    for (int u = 0; u < U; u++) {
+        const uint64_t cu = (uint64_t)u << 8;
+        Tu[u] = xor_cols(tks, cu);
+        pu[u] = __popcll(cu & s.rhoc) & 1;
+    }
+    double a0 = 0, a1 = 0;
+    unsigned int i0, i1;
+    block_range(cx.nchunks, i0, i1);
+    uint64_t bh = 0;
+    int ph = 0;
+    if (i0 < i1) {
+        const uint64_t cb = (uint64_t)(i0 ^ (i0 >> 1)) << cl;
+        bh = xor_cols(tks, cb) ^ Tt;
+        ph = (__popcll(cb & s.rhoc) & 1) ^ pt;
+    }
+    for (unsigned int i = i0; i < i1; i++) {
+        if (i > i0) {
+            const int j = __ffs((int)i) - 1 + cl;
+            bh ^= tks[j];
+            ph ^= (int)((s.rhoc >> j) & 1);
+        }
+        double2 v[U][NTQ];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t b = bh ^ Tu[u];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) v[u][t] = mem[b ^ s.tq[t]];
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const uint64_t b = bh ^ Tu[u];
+            const int pc = ph ^ pu[u];
+            double S[2][2][2] = {};   // [x][tau][re/im]
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                const int t0 = MOUT == 1 ? 0 : s.tau0[t], t1 = MOUT == 1 ? 0 : s.tau1[t];
+                const bool ng = ((pc ^ s.par[t]) & 1) != 0;
+#pragma unroll
+                for (int tau = 0; tau < MOUT; tau++) {
+                    if (t0 == tau) { S[0][tau][0] += v[u][t].x; S[0][tau][1] += v[u][t].y; }
+                    if (t1 == tau) { S[1][tau][0] += ng ? -v[u][t].x : v[u][t].x; S[1][tau][1] += ng ? -v[u][t].y : v[u][t].y; }
+                }
+            }
+#pragma unroll
+            for (int b2 = 0; b2 < (WRITE ? 1 : 2); b2++) {
+                double nn = 0;
+#pragma unroll
+                for (int tau = 0; tau < MOUT; tau++) {
+                    const double r = wr[b2][0] * S[0][tau][0] - wi[b2][0] * S[0][tau][1] + wr[b2][1] * S[1][tau][0] - wi[b2][1] * S[1][tau][1];
+                    const double im = wr[b2][0] * S[0][tau][1] + wi[b2][0] * S[0][tau][0] + wr[b2][1] * S[1][tau][1] + wi[b2][1] * S[1][tau][0];
+                    nn += r * r + im * im;
+                    if (WRITE) mem[tau == 0 ? b : (b ^ s.g)] = make_double2(r, im);
+                }
+                if (b2 == 0) a0 += nn;
+                else a1 += nn;
+            }
+        }
+    }
+    double t0, t1;
+    if (!grid_reduce2(a0, a1, cx, t0, t1)) return;
+    if (WRITE) write_epilogue(cx, s.k, P.bv, t0);
+    else norm_epilogue(cx, s.k, t0, t1);
+}
+
 // Start of a string / sample: the unit table and a fresh state.
 template <typename E>
 __global__ void k_begin(E *mem, DevState *st) {

@@ -57,6 +57,7 @@ def _load():
         "gsb_sample_device": (c.c_int, [P, P, c.c_int64, P, P]),
         "gsb_synchronize": (c.c_int, [P]),
         "gsb_set_stream": (c.c_int, [P, P]),
+        "gsb_set_arith": (c.c_int, [P, c.c_int]),
         "gsb_profile_steps": (c.c_int, [P, i8p, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_launches_per_item": (c.c_int, [P, c.c_int, c.POINTER(c.c_int64)]),
         "gsb_validate_text": (c.c_int, [c.c_char_p, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
@@ -76,7 +77,7 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search")
 
 
@@ -255,6 +256,11 @@ class Engine:
     def set_stream(self, cuda_stream):
         """Queue work on a cudaStream_t (int handle, e.g. torch.cuda.current_stream().cuda_stream); 0 = own."""
         _check(_lib.gsb_set_stream(self.handle, ctypes.c_void_p(int(cuda_stream) or None)))
+
+    def set_arith(self, bits):
+        """complex64 wide-step arithmetic: 32 (FP32 sums and rotation, default) or 64 (exact sums + FP64 rotation,
+        the reference's complex64 arithmetic)."""
+        _check(_lib.gsb_set_arith(self.handle, int(bits)))
 
     def synchronize(self):
         _check(_lib.gsb_synchronize(self.handle))

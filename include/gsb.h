@@ -112,6 +112,11 @@ int gsb_synchronize(gsb_engine *e);
 /* Queue the engine's work on `cuda_stream` (a cudaStream_t of the engine's device; NULL = the engine's own stream),
  * e.g. a framework's current stream, so events recorded there bracket the engine's kernels. */
 int gsb_set_stream(gsb_engine *e, void *cuda_stream);
+/* Arithmetic of a complex64 engine's wide-step kernels (steps of >= 2^11 cosets): 32 (default) sums a coset's
+ * entries and rotates them by M in FP32 (norms and scales stay FP64); 64 sums exactly and rotates in FP64, rounding
+ * only when storing, which is the reference's complex64 arithmetic (slower: the FP64 pipe becomes the limit).
+ * Either way the stored table is complex64.  No effect on a complex128 engine. */
+int gsb_set_arith(gsb_engine *e, int bits);
 
 /* Per-step kernel timing for one forced string: ms_write[k] and ms_norm[k] (0 when a pass does not run) from CUDA
  * events on the engine's stream, mode 0 = 'chain' (one pass per step), 1 = 'prob' (norm + write per step). */

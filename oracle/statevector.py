@@ -66,3 +66,20 @@ def index_of(bits_by_qubit):
     for b in bits_by_qubit:
         idx = 2 * idx + int(b)
     return idx
+
+
+def dense_state_torch(n, ops, device="cuda"):
+    """The same statevector computed with torch (complex128) on `device`, for n up to ~28 (2^n x 16 bytes)."""
+    import torch
+    psi = torch.zeros([2] * n, dtype=torch.complex128, device=device)
+    psi[(0,) * n] = 1
+    for name, qs in ops:
+        if name == "cz":
+            idx = [slice(None)] * n
+            idx[qs[0]] = 1
+            idx[qs[1]] = 1
+            psi[tuple(idx)] *= -1
+        else:
+            G = torch.tensor(gate(name), dtype=torch.complex128, device=device)
+            psi = torch.movedim(torch.tensordot(G, psi, dims=([1], [qs[0]])), 0, qs[0])
+    return psi.reshape(-1)

@@ -1,0 +1,148 @@
+"""Parity of the wide-step kernels (steps of >= 2^10 / 2^11 cosets: the complex128 kernel and the complex64 paired
+kernel) with the oracle, in every executor mode, on an instance wide enough to use them; and complex128 amplitudes
+against a brute-force statevector at n = 24.
+
+Modes: "c128" (complex128 arena), "c64x" (complex64 arena, exact pair sums + FP64 rotation: the oracle's own
+complex64 arithmetic) and "c64" (complex64 arena, FP32 arithmetic, the default).  Tolerances: c128 |d log2 Pr| <=
+1e-9; c64x <= 1e-5; c64 <= 1e-5 x max(1, 2^(-n) / Pr): complex64 rounding is absolute in units of the table norm, so
+a string k times less likely than a typical one (Pr ~ 2^-n) carries k times the relative error.  Sampled bits are
+identical to the oracle's (same mt19937_64 streams).
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+MODES = ["c128", "c64x", "c64"]
+
+
+def engine(path, mode):
+    import gsb
+    e = gsb.Engine(path, precision=128 if mode == "c128" else 64)
+    if mode == "c64x":
+        e.set_arith(64)
+    return e
+
+
+def lp_tol(mode, lp, n):
+    if mode == "c128":
+        return 1e-9
+    if mode == "c64x":
+        return 1e-5
+    return 1e-5 * max(1.0, 2.0 ** (-n - lp))
+
+
+def cond_tol(mode):
+    return {"c128": 1e-10, "c64x": 1e-6, "c64": 1e-5}[mode]
+
+
+@pytest.fixture(scope="module")
+def wide_case():
+    import workloads
+    w = workloads.matching_instance(38, 38, 7, 8, 20000)
+    assert w["width"] >= 14
+    td = tempfile.mkdtemp()
+    path = os.path.join(td, "plan.txt")
+    open(path, "w").write(w["plan"])
+    w["path"] = path
+    return w
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_wide_chain_prob_vs_oracle(wide_case, mode):
+    import workloads
+    from oracle import Oracle
+    ns = n = len(wide_case["steps"])
+    strings = workloads.random_strings(ns, 24, seed=31)
+    o = Oracle(wide_case["path"], 128 if mode == "c128" else 64)
+    with engine(wide_case["path"], mode) as eng:
+        lp, cond = eng.chain(strings)
+        lpp = eng.prob(strings[:6])
+    for i in range(len(strings)):
+        olp, ocond = o.chain1(strings[i])
+        assert abs(lp[i] - olp) <= lp_tol(mode, olp, n), (i, lp[i], olp)
+        if olp > -n - 3:
+            assert np.abs(cond[i] - ocond).max() <= cond_tol(mode)
+    for i in range(6):
+        olp = o.prob(strings[i])
+        assert abs(lpp[i] - olp) <= lp_tol(mode, olp, n)
+    o.close()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_wide_samples_and_hybrid_vs_oracle(wide_case, mode):
+    import gsb
+    import workloads
+    from oracle import Oracle
+    ns = n = len(wide_case["steps"])
+    o = Oracle(wide_case["path"], 128 if mode == "c128" else 64)
+    with engine(wide_case["path"], mode) as eng:
+        for seeding, seed in ((gsb.SEED_INT, 77), (gsb.SEED_SEQ, 78)):
+            bits, lp = eng.sample(6, seed, seeding=seeding)
+            for i in range(6):
+                ob, olp = o.sample(seeding, seed, i)
+                assert list(bits[i]) == list(ob) and abs(lp[i] - olp) <= lp_tol(mode, olp, n)
+        lines = []
+        base = workloads.random_strings(ns, 4, seed=5)
+        for i in range(4):
+            s = "".join(str(int(b)) for b in base[i])
+            lines.append(s[:ns - 6] + "?" * 6)
+        hb, hlp, hc = eng.hybrid(lines, 11)
+        for i, ln in enumerate(lines):
+            ob, olp, oc = o.hybrid(ln, 11, i)
+            assert list(hb[i]) == list(ob) and abs(hlp[i] - olp) <= lp_tol(mode, olp, n)
+            if olp > -n - 3:
+                assert np.abs(hc[i] - oc).max() <= cond_tol(mode)
+    o.close()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_wide_prefix_resume_two_slices(wide_case, mode):
+    """prefix dump at a wide step, then resume over two half tables (the slice sum of gsamp2.cpp:196-205)."""
+    import workloads
+    from oracle import Oracle
+    prec = 128 if mode == "c128" else 64
+    ns = n = len(wide_case["steps"])
+    K = max(range(ns), key=lambda k: wide_case["steps"][k]["r"])
+    s = "".join(str(int(b)) for b in workloads.random_strings(ns, 1, seed=6)[0])
+    line = s[:K] + "?" * (ns - K)
+    o = Oracle(wide_case["path"], prec)
+    with engine(wide_case["path"], mode) as eng:
+        d, ls, lp = eng.prefix(line, K)
+        od, ols, olp = o.prefix(line, K)
+        assert abs(lp - olp) <= lp_tol(mode, olp, K) and abs(ls - ols) <= 1e-6
+        scale = max(1e-300, np.abs(od).max())
+        assert np.abs(d.astype(np.complex128) - od).max() <= (1e-12 if prec == 128 else 1e-5) * scale
+        half = (d / 2).astype(d.dtype)
+        bits, lpf, lpp, cond = eng.resume(line, K, 21, 0, [half, half], [ls, ls])
+        ob, olpf, olpp, oc = o.resume(line, K, 21, 0, [half.astype(np.complex128)] * 2, [ls, ls])
+    assert list(bits) == list(ob)
+    assert abs(lpf - olpf) <= lp_tol(mode, olpf, n) and abs(lpp - olpp) <= 1e-9
+    assert np.abs(cond[K:] - oc[K:]).max() <= cond_tol(mode)
+    o.close()
+
+
+def test_statevector_n24():
+    """complex128 amplitudes of 64 strings of an n = 24 random-matching circuit against a brute-force 2^24
+    statevector (simulated with torch on the GPU): |d Pr| <= 1e-12 absolute, |d log2 Pr| <= 1e-9."""
+    import gsb
+    import workloads
+    from oracle import statevector
+    w = workloads.matching_instance(24, 24, 5, 6, 20000)
+    psi = statevector.dense_state_torch(24, list(w["body"]) + list(w["tail"]), device="cuda")
+    p = (psi.abs() ** 2).cpu().numpy()
+    rng = np.random.default_rng(3)
+    idx = list(rng.integers(0, 1 << 24, 56)) + list(np.argsort(p)[-8:])
+    strings = []
+    for ix in idx:
+        bits = [(int(ix) >> (23 - q)) & 1 for q in range(24)]
+        strings.append([bits[s["v"]] for s in w["steps"]])
+    with gsb.Engine.from_text(w["plan"], precision=128) as eng:
+        lp = eng.chain(np.array(strings, np.int8))[0]
+    ref = p[idx]
+    assert np.abs(np.exp2(lp) - ref).max() <= 1e-12
+    big = ref > 1e-10                   # log2 amplifies the absolute rounding of very unlikely strings
+    assert big.sum() >= 48 and np.abs(lp[big] - np.log2(ref[big])).max() <= 1e-9
