@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "gsb.h"
+#include "gsb_common.h"
 #include "gsb_kernels.cuh"
 #include "gsb_plan.h"
 
@@ -25,7 +26,7 @@ namespace gsb {
 
 static thread_local std::string g_err;
 
-static int fail(int code, const std::string &msg) {
+int fail(int code, const std::string &msg) {
     g_err = msg;
     return code;
 }
@@ -585,7 +586,7 @@ int gsb_prefix(gsb_engine *e, const int8_t *forced, int K, void *dump, double *l
     if (!e) return fail(GSB_E_STATE, "null engine");
     Engine *E = eng(e);
     const int ns = E->plan.ns;
-    if (!forced || !dump || K < 0) return fail(GSB_E_USAGE, "bad argument");
+    if (!forced || K < 0) return fail(GSB_E_USAGE, "bad argument");
     for (int k = 0; k < std::min(K, ns); k++)
         if (forced[k] < 0) return fail(GSB_E_PREFIX_FREE, "'?' before K in prefix mode");
         else if (forced[k] > 1) return fail(GSB_E_USAGE, "bits must be 0 or 1");
@@ -597,17 +598,19 @@ int gsb_prefix(gsb_engine *e, const int8_t *forced, int K, void *dump, double *l
     k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
     GSB_CK(E->launch_begin());
     for (int k = 0; k < Kr; k++) GSB_CK(E->launch_step(k, true, DRV_HYBRID, Kr, true, false));
-    int nk, ntq;
-    gsb_dump_shape(e, K, &nk, &ntq);
-    const size_t nent = ((size_t)1 << nk) * (size_t)ntq, bytes = nent * E->esize;
-    int rc = ensure_dump(E, bytes);
-    if (rc) return rc;
-    StepArgs a = dump_args(E, K);
-    const int grid = (int)std::min<size_t>((nent + 255) / 256, (size_t)E->sms * 8);
-    if (E->prec == 128) k_gather<double2><<<grid, 256, 0, E->stream>>>(a, (const double2 *)E->mem, ntq, (double2 *)E->d_dump);
-    else k_gather<float2><<<grid, 256, 0, E->stream>>>(a, (const float2 *)E->mem, ntq, (float2 *)E->d_dump);
-    GSB_CK(cudaGetLastError());
-    GSB_CK(cudaMemcpyAsync(dump, E->d_dump, bytes, cudaMemcpyDeviceToHost, E->stream));
+    if (dump) {   // dump == NULL: only the prefix probability (a marginal) is wanted
+        int nk, ntq;
+        gsb_dump_shape(e, K, &nk, &ntq);
+        const size_t nent = ((size_t)1 << nk) * (size_t)ntq, bytes = nent * E->esize;
+        int rc = ensure_dump(E, bytes);
+        if (rc) return rc;
+        StepArgs a = dump_args(E, K);
+        const int grid = (int)std::min<size_t>((nent + 255) / 256, (size_t)E->sms * 8);
+        if (E->prec == 128) k_gather<double2><<<grid, 256, 0, E->stream>>>(a, (const double2 *)E->mem, ntq, (double2 *)E->d_dump);
+        else k_gather<float2><<<grid, 256, 0, E->stream>>>(a, (const float2 *)E->mem, ntq, (float2 *)E->d_dump);
+        GSB_CK(cudaGetLastError());
+        GSB_CK(cudaMemcpyAsync(dump, E->d_dump, bytes, cudaMemcpyDeviceToHost, E->stream));
+    }
     DevState hs;
     GSB_CK(cudaMemcpyAsync(&hs, E->st, sizeof hs, cudaMemcpyDeviceToHost, E->stream));
     GSB_CK(cudaStreamSynchronize(E->stream));
@@ -776,6 +779,26 @@ int gsb_set_arith(gsb_engine *e, int bits) {
         E->lw[(size_t)k] = E->shape(E->args[(size_t)k], true);
         E->ln[(size_t)k] = E->shape(E->args[(size_t)k], false);
     }
+    return 0;
+}
+
+int gsb_set_matrices(gsb_engine *e, const double *M) {
+    if (!e || !M) return fail(GSB_E_USAGE, "null argument");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    for (int k = 0; k < E->plan.ns; k++) {
+        HStep &s = E->plan.st[(size_t)k];
+        StepArgs &a = E->args[(size_t)k];
+        for (int b = 0; b < 2; b++)
+            for (int x = 0; x < 2; x++) {
+                const double re = M[(size_t)k * 8 + (size_t)(4 * b + 2 * x)], im = M[(size_t)k * 8 + (size_t)(4 * b + 2 * x + 1)];
+                s.Mr[b][x] = a.Mr[b][x] = re;
+                s.Mi[b][x] = a.Mi[b][x] = im;
+            }
+    }
+    for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);   // the captured graphs hold M by value
+    E->graphs.clear();
     return 0;
 }
 

@@ -58,8 +58,14 @@ def _load():
         "gsb_synchronize": (c.c_int, [P]),
         "gsb_set_stream": (c.c_int, [P, P]),
         "gsb_set_arith": (c.c_int, [P, c.c_int]),
+        "gsb_set_matrices": (c.c_int, [P, dp]),
         "gsb_profile_steps": (c.c_int, [P, i8p, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_launches_per_item": (c.c_int, [P, c.c_int, c.POINTER(c.c_int64)]),
+        "gsb_dp_open_text": (c.c_int, [c.c_char_p, c.c_size_t, c.c_int, c.c_int, c.POINTER(P)]),
+        "gsb_dp_close": (c.c_int, [P]),
+        "gsb_dp_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+        "gsb_dp_run": (c.c_int, [P, c.c_int64, dp, dp, dp]),
+        "gsb_dp_extend": (c.c_int, [c.c_int, c.c_int, c.c_uint64, c.c_uint64, c.c_int, u64p, dp, dp, dp, c.c_int]),
         "gsb_validate_text": (c.c_int, [c.c_char_p, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
                                         c.POINTER(c.c_int)]),
         "gsb_cut_profile": (c.c_int, [c.c_int, c.POINTER(c.c_uint8), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
@@ -77,8 +83,9 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
-           "gsb_cut_profile", "gsb_order_search")
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
+           "gsb_dp_extend")
 
 
 def lib():
@@ -121,11 +128,12 @@ class Engine:
 
     def __init__(self, plan_path=None, precision=GSB_C64, device=0, text=None):
         h = ctypes.c_void_p()
-        if text is not None:
-            b = text.encode() if isinstance(text, str) else bytes(text)
-            _check(_lib.gsb_open_text(b, len(b), int(precision), int(device), ctypes.byref(h)))
-        else:
-            _check(_lib.gsb_open_file(os.fsencode(plan_path), int(precision), int(device), ctypes.byref(h)))
+        if text is None:
+            with open(plan_path) as f:
+                text = f.read()
+        self.plan_text = text if isinstance(text, str) else bytes(text).decode()
+        b = self.plan_text.encode()
+        _check(_lib.gsb_open_text(b, len(b), int(precision), int(device), ctypes.byref(h)))
         self._h = h
         n, ns, R, p = (ctypes.c_int() for _ in range(4))
         _check(_lib.gsb_info(h, ctypes.byref(n), ctypes.byref(ns), ctypes.byref(R), ctypes.byref(p)))
@@ -216,13 +224,17 @@ class Engine:
         _check(_lib.gsb_dump_shape(self.handle, int(K), ctypes.byref(nk), ctypes.byref(ntq)))
         return nk.value, ntq.value
 
-    def prefix(self, string, K):
-        """'prefix': (dump [2^nk * ntq] of the arena dtype in (c, tq) order, logscale, log2 Pr(prefix))."""
+    def prefix(self, string, K, want_dump=True):
+        """'prefix': (dump [2^nk * ntq] of the arena dtype in (c, tq) order, logscale, log2 Pr(prefix)).
+        With want_dump=False only (None, logscale, log2 Pr of the first K steps) -- a marginal probability."""
         f = as_bits([string], self.ns, allow_free=True)[0].copy()
-        nk, ntq = self.dump_shape(K)
-        dump = np.zeros((1 << nk) * ntq, self.entry_dtype)
+        dump = None
+        if want_dump:
+            nk, ntq = self.dump_shape(K)
+            dump = np.zeros((1 << nk) * ntq, self.entry_dtype)
         ls, lp = ctypes.c_double(), ctypes.c_double()
-        _check(_lib.gsb_prefix(self.handle, _ptr(f, ctypes.c_int8), int(K), dump.ctypes.data_as(ctypes.c_void_p),
+        _check(_lib.gsb_prefix(self.handle, _ptr(f, ctypes.c_int8), int(K),
+                               None if dump is None else dump.ctypes.data_as(ctypes.c_void_p),
                                ctypes.byref(ls), ctypes.byref(lp)))
         return dump, ls.value, lp.value
 
@@ -257,6 +269,16 @@ class Engine:
         """Queue work on a cudaStream_t (int handle, e.g. torch.cuda.current_stream().cuda_stream); 0 = own."""
         _check(_lib.gsb_set_stream(self.handle, ctypes.c_void_p(int(cuda_stream) or None)))
 
+    def set_matrices_from_text(self, plan_text):
+        """Load the M matrices of another plan with this plan's layout (a slice plan) into this engine."""
+        rows = [ln.split() for ln in plan_text.strip().split("\n")]
+        mine = [ln.split() for ln in self.plan_text.strip().split("\n")]
+        if len(rows) != len(mine) or rows[0] != mine[0] or any(a[:-8] != b[:-8] for a, b in zip(rows[1:], mine[1:])):
+            raise ValueError("the plan's layout differs from this engine's (only M may differ)")
+        rows = rows[1:]
+        M = np.array([[float(x) for x in r[-8:]] for r in rows], np.float64).reshape(-1)
+        _check(_lib.gsb_set_matrices(self.handle, _ptr(np.ascontiguousarray(M), ctypes.c_double)))
+
     def set_arith(self, bits):
         """complex64 wide-step arithmetic: 32 (FP32 sums and rotation, default) or 64 (exact sums + FP64 rotation,
         the reference's complex64 arithmetic)."""
@@ -278,6 +300,64 @@ class Engine:
         n = ctypes.c_int64()
         _check(_lib.gsb_launches_per_item(self.handle, int(mode), ctypes.byref(n)))
         return n.value
+
+
+class DpEngine:
+    """The out-of-place amplitude engine (the reference's dp.cpp) on one plan: complex amplitudes Z(w)."""
+
+    def __init__(self, plan_text, precision=GSB_C128, device=0):
+        h = ctypes.c_void_p()
+        b = plan_text.encode() if isinstance(plan_text, str) else bytes(plan_text)
+        _check(_lib.gsb_dp_open_text(b, len(b), int(precision), int(device), ctypes.byref(h)))
+        self._h = h
+        m, ns, mr = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.gsb_dp_info(h, ctypes.byref(m), ctypes.byref(ns), ctypes.byref(mr)))
+        self.m, self.ns, self.maxr = m.value, ns.value, mr.value
+
+    def run(self, slices):
+        """sum over slices (pre, weights [(w0, w1) per vertex]) of pre * Z(weights) (one reference job)."""
+        pre = np.zeros(2 * max(len(slices), 1))
+        w = np.zeros(max(len(slices), 1) * max(self.m, 1) * 4)
+        for i, (p, ww) in enumerate(slices):
+            pre[2 * i], pre[2 * i + 1] = complex(p).real, complex(p).imag
+            for q, (a, b) in enumerate(ww):
+                j = (i * self.m + q) * 4
+                w[j:j + 4] = complex(a).real, complex(a).imag, complex(b).real, complex(b).imag
+        out = np.zeros(2)
+        _check(_lib.gsb_dp_run(self._h, len(slices), _ptr(pre, ctypes.c_double), _ptr(w, ctypes.c_double),
+                               _ptr(out, ctypes.c_double)))
+        return complex(out[0], out[1])
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.gsb_dp_close(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def dp_extend(old, r, rn, rho, piv, ker, wv, device=0):
+    """One out-of-place DP step on the GPU (complex128): new table of 2^rn entries."""
+    old = np.ascontiguousarray(old, np.complex128)
+    assert old.shape == (1 << r,)
+    out = np.zeros(1 << rn, np.complex128)
+    k = np.ascontiguousarray(list(ker) or [0], np.uint64)
+    w = np.array([complex(wv[0]).real, complex(wv[0]).imag, complex(wv[1]).real, complex(wv[1]).imag])
+    pm = sum(1 << p for p in piv)
+    _check(_lib.gsb_dp_extend(int(r), int(rn), int(rho), int(pm), len(ker), _ptr(k, ctypes.c_uint64),
+                              _ptr(w, ctypes.c_double), _ptr(old.view(np.float64), ctypes.c_double),
+                              _ptr(out.view(np.float64), ctypes.c_double), int(device)))
+    return out
 
 
 def validate_text(text):

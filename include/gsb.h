@@ -93,7 +93,7 @@ int gsb_dump_shape(const gsb_engine *e, int K, int *nk, int *ntq);
 
 /* 'prefix': run the forced steps 0..K-1 of one string and copy out the live table in logical (c, tq) order, entries
  * of the arena type (complex64 = 2 floats, complex128 = 2 doubles); *logscale and log2 Pr(prefix) as the reference
- * prints them (gsamp2.cpp:162-175). */
+ * prints them (gsamp2.cpp:162-175).  dump may be NULL when only log2 Pr(prefix) (a marginal) is wanted. */
 int gsb_prefix(gsb_engine *e, const int8_t *forced, int K, void *dump, double *logscale, double *log2p_prefix);
 
 /* 'resume': sum nslices dump tables (scaled by 2^(logscale_s - max)), read through the optional twist translation
@@ -112,6 +112,10 @@ int gsb_synchronize(gsb_engine *e);
 /* Queue the engine's work on `cuda_stream` (a cudaStream_t of the engine's device; NULL = the engine's own stream),
  * e.g. a framework's current stream, so events recorded there bracket the engine's kernels. */
 int gsb_set_stream(gsb_engine *e, void *cuda_stream);
+/* Replace every step's rotation matrix: M is [nsteps][2][2] complex (re, im), M[k][b][x] as the plan text lists
+ * it.  The layout stays; this is how one engine (one arena) serves all slice plans of make_sliced_plans, which
+ * share the layout and differ only in M (sliced_plans.py:1-14). */
+int gsb_set_matrices(gsb_engine *e, const double *M);
 /* Arithmetic of a complex64 engine's wide-step kernels (steps of >= 2^11 cosets): 32 (default) sums a coset's
  * entries and rotates them by M in FP32 (norms and scales stay FP64); 64 sums exactly and rotates in FP64, rounding
  * only when storing, which is the reference's complex64 arithmetic (slower: the FP64 pipe becomes the limit).
@@ -124,6 +128,22 @@ int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_wri
 
 /* Number of kernel launches one string / sample makes in the given mode (0 chain, 1 prob/sample, 2 hybrid). */
 int gsb_launches_per_item(const gsb_engine *e, int mode, int64_t *launches);
+
+/* ---- out-of-place amplitude engine (the reference's dp.cpp, dp.cpp:14-63) ----
+ * Plan text as engine.py:5-12 writes it ("m nsteps maxr", then "v r rn rho pivmask nker ker..." per step).  Two
+ * tables of 2^maxr entries, complex128 (precision 128) or complex64 storage with FP64 arithmetic (64, the reference's
+ * -DDP_FLOAT build). */
+typedef struct gsb_dp gsb_dp;
+int gsb_dp_open_text(const char *plan_text, size_t len, int precision, int device, gsb_dp **out);
+int gsb_dp_close(gsb_dp *d);
+int gsb_dp_info(const gsb_dp *d, int *m, int *nsteps, int *maxr);
+/* One job (dp.cpp:35-61): out = sum over slices of pre[s] * Z(w[s]); pre is [nslices] complex (re, im), w is
+ * [nslices][m] x (w0 re, w0 im, w1 re, w1 im); out is one complex (re, im). */
+int gsb_dp_run(gsb_dp *d, int64_t nslices, const double *pre, const double *w, double *out);
+/* One out-of-place step on a host table (complex128): new[c'] for c' < 2^rn from old[2^r] with weights
+ * wv = (w0 re, w0 im, w1 re, w1 im) (sampler_ref.py:8-23 `extend`, ref.py:18-31). */
+int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker, const double *wv,
+                  const double *old_table, double *new_table, int device);
 
 /* ---- host-side helpers (no GPU needed) ---- */
 

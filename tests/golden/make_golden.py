@@ -16,12 +16,16 @@ with this repository's modules of the same names:
             width-30 plan regenerated from its #151 circuit and order (w30/nq70_inplace_plan_regen.txt).
   executor  (compiled reference executor, oracle/_ref)  gsamp2 outputs on small plans: prob / chain on every
             string (complex128 and complex64 builds), sample / sample2 / hybrid lines, a prefix + resume run.
+  extras    (reference on sys.path + oracle/_ref/dp)  engine.py plan/jobs with vertex slicing and dp.cpp's
+            amplitudes, ref.run amplitudes, sampler_ref conditionals / samples / extend / chain_distribution, and
+            make_sliced_plans slice plans with their twist files.
 
 Reference data files copied verbatim (the pinned width-30 instance and its published outputs):
   w30/nq70.qasm, w30/order_w30.json, w30/nq70_inplace_plan.txt (as shipped), w30/gate_strings.txt,
   w30/ibm_strings_64.txt + w30/ibm_log2p_64.txt + w30/ibm_chain_64.txt (first 64 of 1,726 IBM shots),
   w30/laptop_samples_w30.txt, w30/samples2_16.txt (first 16 'sample2' samples), w30/rngbits_2000000.txt.
 """
+import itertools
 import json
 import os
 import random
@@ -205,6 +209,122 @@ def copy_w30():
               open(os.path.join(d, "gate_log2p.json"), "w"))
 
 
+def phase_extras(exp, out):
+    """Reference outputs of the rows around the executor: dp.cpp jobs with slicing (engine.py), sampler_ref, and
+    make_sliced_plans with a twist file."""
+    sys.path.insert(0, REF)
+    import numpy as np
+    from tableau import Tableau
+    from amp import Amplitudes
+    from engine import Sliced, write_plan, write_jobs
+    from ref import run
+    import sampler_ref
+    from sliced_plans import make_sliced_plans
+    data = json.load(open(exp))
+    cases = [c for c in data["cases"] if c["name"].startswith("small") and c["n"] >= 5 and all(
+        t[0] in ("tdg", "h") or t[0].startswith("rz(") for t in c["tail"])][:6]
+    res = dict(dp=[], sampler=[], sliced=[])
+    with tempfile.TemporaryDirectory() as td:
+        for c in cases:
+            n = c["n"]
+            T = Tableau(n)
+            for g, qs in c["body"]:
+                T.apply(g, qs)
+            am = Amplitudes(n, T, [tuple(t) for t in c["tail"]], c["order"])
+            rr = random.Random(n * 101)
+            S = sorted(rr.sample(range(n), 2))
+            sl = Sliced(am.A, c["order"], S)
+            bs = [[rr.randrange(2) for _ in range(n)] for _ in range(3)]
+            ws = [am.weights(b) for b in bs]
+            write_plan(os.path.join(td, "dp_plan.txt"), sl.steps, sl.m)
+            write_jobs(os.path.join(td, "dp_jobs.txt"), sl, ws)
+            lines = subprocess.run([os.path.join(ROOT, "oracle", "_ref", "dp"), "dp_plan.txt", "dp_jobs.txt"],
+                                   capture_output=True, text=True, cwd=td, check=True).stdout.split("\n")
+            res["dp"].append(dict(name=c["name"], S=S, bits=bs, plan=open(os.path.join(td, "dp_plan.txt")).read(),
+                                  jobs=open(os.path.join(td, "dp_jobs.txt")).read(),
+                                  ref_dp=[ln for ln in lines if ln.strip()],
+                                  ref_run=[[run(am.steps, w).real, run(am.steps, w).imag] for w in ws]))
+            prefs = [[rr.randrange(2) for _ in range(t)] for t in (0, 1, n // 2, n - 1)]
+            conds = [[list(map(float, x)) for x in sampler_ref.conditionals(am, p)] for p in prefs]
+            samples = [sampler_ref.sample(am, np.random.default_rng(seed)) for seed in (1, 2, 3, 4)]
+            st0 = am.steps[min(2, n - 1)]
+            old = np.array([complex(rr.gauss(0, 1), rr.gauss(0, 1)) for _ in range(1 << st0["r"])])
+            wv = (am.M[st0["v"]][0, 0], am.M[st0["v"]][0, 1])
+            ext = sampler_ref.extend(old, st0, wv)
+            dist = sampler_ref.chain_distribution(am) if n <= 7 else None
+            res["sampler"].append(dict(name=c["name"], prefixes=prefs, conditionals=conds, samples=samples,
+                                       extend_step=min(2, n - 1),
+                                       extend_in=[[z.real, z.imag] for z in old],
+                                       extend_out=[[z.real, z.imag] for z in ext],
+                                       chain_distribution=None if dist is None else
+                                       [["".join(map(str, k)), v] for k, v in sorted(dist.items())]))
+        # sliced plans with a suffix neighbour: the first case whose slice vertices have suffix neighbours
+        for c in data["cases"]:
+            if not c["name"].startswith("small") or c["n"] < 7 or any(t[0].startswith("u3(") for t in c["tail"]):
+                continue
+            n = c["n"]
+            T = Tableau(n)
+            for g, qs in c["body"]:
+                T.apply(g, qs)
+            am = Amplitudes(n, T, [tuple(t) for t in c["tail"]], c["order"])
+            order = c["order"]
+            K = n - 2
+            S = [order[1]]
+            try:
+                info = make_sliced_plans(am.A, [m.copy() for m in am.M], order, S, os.path.join(td, "sp"), K=K, ND=n)
+            except AssertionError:
+                continue
+            if not info["twist"]:
+                continue
+            files = {}
+            for bits in itertools.product([0, 1], repeat=len(S)):
+                tag = "".join(map(str, bits))
+                files[tag] = open(os.path.join(td, f"sp_s{tag}.txt")).read()
+            res["sliced"].append(dict(name=c["name"], S=S, K=K, info=info, plans=files,
+                                      twist=open(os.path.join(td, "sp_twist.txt")).read(),
+                                      slices_json=open(os.path.join(td, "sp_slices.json")).read()))
+            if len(res["sliced"]) >= 3:
+                break
+        # the reference's hybrid rejection driver (doped_sampler.py) run on an undoped instance (--na 0 --nd n)
+        # with the compiled reference executor as --bin: unsliced sample + score, and the sliced variant
+        res["driver"] = []
+        gs2 = os.path.join(ROOT, "oracle", "_ref", "gsamp2")
+        for d in res["sliced"][:1]:
+            c = {x["name"]: x for x in data["cases"]}[d["name"]]
+            n = c["n"]
+            T = Tableau(n)
+            for g, qs in c["body"]:
+                T.apply(g, qs)
+            am = Amplitudes(n, T, [tuple(t) for t in c["tail"]], c["order"])
+            from inplace import plan_inplace as _pi, write_inplace_plan as _wi
+            R = max(1, max(max(st["r"], st["rn"]) for st in am.steps))
+            _wi(os.path.join(td, "full.txt"), _pi(am.A, c["order"], R), R, am.M, n)
+            json.dump(c["order"], open(os.path.join(td, "sv.json"), "w"))
+            for tag, text in d["plans"].items():
+                open(os.path.join(td, f"sl_s{tag}.txt"), "w").write(text)
+            open(os.path.join(td, "sl_twist.txt"), "w").write(d["twist"])
+            rr = random.Random(7)
+            strings = ["".join(str(rr.randrange(2)) for _ in range(n)) for _ in range(6)]
+            open(os.path.join(td, "str.txt"), "w").write("\n".join(strings) + "\n")
+            drv = os.path.join(REF, "doped_sampler.py")
+            common = ["--na", "0", "--nd", str(n), "--bin", gs2, "--threads", "2"]
+            runs = {}
+            for name, args in (("sample", ["sample", "full.txt", "sv.json", "24", "5", "2.0", "o_sample.txt", "--m", "2"]),
+                               ("score", ["score", "full.txt", "sv.json", "str.txt", "o_score.txt"]),
+                               ("sample_sliced", ["sample", "sl_s0.txt", "sv.json", "12", "6", "2.0", "o_ss.txt",
+                                                  "--slices", "sl_s0.txt,sl_s1.txt", "--K", str(d["K"]), "--twist",
+                                                  "sl_twist.txt", "--m", "2"]),
+                               ("score_sliced", ["score", "sl_s0.txt", "sv.json", "str.txt", "o_sc.txt", "--slices",
+                                                 "sl_s0.txt,sl_s1.txt", "--K", str(d["K"]), "--twist", "sl_twist.txt"])):
+                outf = args[args.index("sv.json") + (4 if args[0] == "sample" else 2)]
+                if os.path.exists(os.path.join(td, outf)):
+                    os.unlink(os.path.join(td, outf))
+                subprocess.run([sys.executable, drv] + args + common, cwd=td, check=True, capture_output=True)
+                runs[name] = dict(args=args, lines=open(os.path.join(td, outf)).read().split("\n"))
+            res["driver"].append(dict(name=d["name"], strings=strings, K=d["K"], runs=runs))
+    json.dump(res, open(out, "w"))
+
+
 def w30_reference_outputs():
     """The compiled reference executor (complex64 and complex128 builds) on the width-30 gate strings: 'prob' and
     'chain' lines for the shipped plan and 'prob' for the regenerated one (about a minute per run on 8 cores)."""
@@ -229,6 +349,8 @@ if __name__ == "__main__":
             phase_expected(sys.argv[3], sys.argv[4])
         elif ph == "executor":
             phase_executor(sys.argv[3], sys.argv[4])
+        elif ph == "extras":
+            phase_extras(sys.argv[3], sys.argv[4])
         sys.exit(0)
     me = os.path.abspath(__file__)
     os.makedirs(os.path.join(HERE, "w30"), exist_ok=True)
@@ -239,5 +361,7 @@ if __name__ == "__main__":
                        check=True, cwd=td)
         subprocess.run([sys.executable, me, "--phase", "executor", os.path.join(HERE, "planner_cases.json"),
                         os.path.join(HERE, "executor_cases.json")], check=True, cwd=td)
+        subprocess.run([sys.executable, me, "--phase", "extras", os.path.join(HERE, "planner_cases.json"),
+                        os.path.join(HERE, "extras_cases.json")], check=True, cwd=td)
     copy_w30()
     print("golden fixtures written to", HERE)

@@ -127,3 +127,45 @@ def test_native_cut_profile_and_order_search(planner_cases):
     A = np.array([[int(ch) for ch in row] for row in c1["A"]], np.uint8)
     order, w = gsb.order_search(A, seed=11, ngreedy=4, iters=20000)
     assert sorted(order) == list(range(20)) and w == max(gsb.cut_profile(A, order)) and w <= 10
+
+
+def _am_of(case):
+    from amp import Amplitudes
+    from circuits import tableau_of
+    return Amplitudes(case["n"], tableau_of(case["n"], case["body"]), [tuple(t) for t in case["tail"]], case["order"])
+
+
+def test_engine_plan_and_jobs_text(planner_cases, tmp_path):
+    """engine.write_plan / Sliced / write_jobs write the reference's text byte for byte (engine.py:5-45)."""
+    import json
+    from conftest import GOLDEN
+    from engine import Sliced, write_jobs, write_plan
+    extras = json.load(open(os.path.join(GOLDEN, "extras_cases.json")))
+    cases = {c["name"]: c for c in planner_cases["cases"]}
+    for d in extras["dp"]:
+        am = _am_of(cases[d["name"]])
+        sl = Sliced(am.A, cases[d["name"]]["order"], d["S"])
+        write_plan(str(tmp_path / "p.txt"), sl.steps, sl.m)
+        write_jobs(str(tmp_path / "j.txt"), sl, [am.weights(b) for b in d["bits"]])
+        assert (tmp_path / "p.txt").read_text() == d["plan"]
+        assert (tmp_path / "j.txt").read_text() == d["jobs"]
+
+
+def test_sliced_plans_and_twist(planner_cases, tmp_path):
+    """make_sliced_plans writes the reference's slice plans, twist file and summary (sliced_plans.py:41-86)."""
+    import json
+    from conftest import GOLDEN
+    from sliced_plans import make_sliced_plans
+    extras = json.load(open(os.path.join(GOLDEN, "extras_cases.json")))
+    cases = {c["name"]: c for c in planner_cases["cases"]}
+    assert extras["sliced"]
+    for d in extras["sliced"]:
+        c = cases[d["name"]]
+        am = _am_of(c)
+        out = str(tmp_path / "sp")
+        info = make_sliced_plans(am.A, [m.copy() for m in am.M], c["order"], d["S"], out, K=d["K"], ND=c["n"])
+        assert info == d["info"]
+        for tag, text in d["plans"].items():
+            assert open(f"{out}_s{tag}.txt").read() == text
+        assert open(f"{out}_twist.txt").read() == d["twist"]
+        assert open(f"{out}_slices.json").read() == d["slices_json"]
