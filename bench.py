@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--arith", type=int, default=32, choices=[32, 64],
                     help="arithmetic of the complex64 wide-step kernels (32: FP32; 64: exact sums + FP64 rotation)")
+    ap.add_argument("--fusion", type=int, default=2, choices=[1, 2, 3],
+                    help="'chain' mode: DP steps fused into one pass over the arena (1 = none)")
     ap.add_argument("--profile-chain", type=int, default=0, metavar="N",
                     help="only evaluate N strings in chain mode on --profile-workload (for ncu captures)")
     ap.add_argument("--profile-workload", default="n70", choices=["n70", "n62"])
@@ -67,6 +69,7 @@ def profile_chain(args):
     w = workloads.matching_n70_w30() if args.profile_workload == "n70" else workloads.matching_instance(62, 62, 3, 13)
     with gsb.Engine.from_text(w["plan"], precision=args.profile_precision) as eng:
         eng.set_arith(args.arith)
+        eng.set_fusion(args.fusion)
         lp, _ = eng.chain(workloads.random_strings(len(w["steps"]), args.profile_chain, seed=9))
     print(json.dumps({"workload": w["name"], "width": w["width"], "log2p": [float(x) for x in lp]}))
 
@@ -222,6 +225,7 @@ def run_gsb(args):
 
     eng = gsb.Engine.from_text(w["plan"], precision=64, device=local)
     eng.set_arith(args.arith)
+    eng.set_fusion(args.fusion)
     stream = torch.cuda.Stream()                  # a real stream: the engine's kernels and the events share it
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
@@ -283,34 +287,42 @@ def run_gsb(args):
     s_per_sample64 = max_over_ranks(e0.elapsed_time(e1) / 1000.0 / S, world)
     sbits64 = d_sb.cpu().numpy()
 
-    # roofline of the dominant kernel (the write pass, k_step<float2,...,true>): per-step event timing
+    # roofline of the dominant kernels (the chain-mode passes: fused groups k_group and single steps), timed per
+    # pass with CUDA events; bytes = the table entries each executed pass must read and write (fused groups keep
+    # their intermediate tables in shared memory, so they move fewer bytes than the unfused step model)
     tot_bytes, per = workloads.pass_bytes(steps, 8, "chain")
+    glen, gent = eng.fusion_groups()
     wsum = np.zeros(ns)
     nprof = 3
     for j in range(nprof):
         wm, _ = eng.profile_steps(strings[j])
         wsum += wm
     wmean = wsum / nprof
-    bytes_w = sum(p[0] for p in per)
-    achieved = bytes_w / (wmean.sum() / 1000.0) / 1e9
-    # per-step detail of the widest steps
-    wide = [k for k in range(ns) if steps[k]["r"] >= 27]
-    wide_bytes = sum(per[k][0] for k in wide)
-    wide_ms = float(wmean[wide].sum())
+    pass_bytes = float(np.sum(gent)) * 8
+    kernel_ms = float(wmean.sum())
+    achieved = pass_bytes / (kernel_ms / 1000.0) / 1e9
+    fused = [k for k in range(ns) if glen[k] >= 2]
+    fused_bytes = float(sum(gent[k] for k in fused)) * 8
+    fused_ms = float(sum(wmean[k] for k in fused))
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "write_pass_traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get("dram_bytes_per_string_c64")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_step<float2,*,*,*,write>",
-                "algorithmic_bytes_per_string": bytes_w, "kernel_ms_per_string": float(wmean.sum()),
-                "wide_steps_frac": (wide_bytes / (wide_ms / 1000.0) / 1e9) / hbm_peak if wide_ms > 0 else None}
+                "traffic": traffic, "peak_kind": peak_kind,
+                "kernel": "chain passes: k_group<float2,float,*> (fused) + k_pair64/k_step (single steps)",
+                "pass_bytes_per_string": pass_bytes, "kernel_ms_per_string": kernel_ms,
+                "fused_passes_frac": (fused_bytes / (fused_ms / 1000.0) / 1e9) / hbm_peak if fused_ms > 0 else None,
+                "unfused_model_bytes_per_string": float(sum(p[0] for p in per)),
+                "unfused_model_GBps": float(sum(p[0] for p in per)) / (kernel_ms / 1000.0) / 1e9,
+                "passes_per_string": int(sum(1 for x in glen if x > 0)), "fusion": args.fusion}
     eng.close()
 
     # complex128 plain form on the first strings of the timed batch, and the c64-vs-c128 agreement
     c128 = {}
     if args.c128_amps > 0:
         e128 = gsb.Engine.from_text(w["plan"], precision=128, device=local)
+        e128.set_fusion(args.fusion)
         e128.set_stream(stream.cuda_stream)
         B = args.c128_amps
         d_lp128 = torch.empty(B, dtype=torch.float64, device="cuda")
@@ -338,13 +350,14 @@ def run_gsb(args):
                 "s_per_sample": s_per_sample128, "max_abs_dlog2p_c64_vs_c128": dlp,
                 "max_abs_dcond_c64_vs_c128": dcond, "samples_same_bits_c64_c128": same_bits}
 
-    launches = (ns + 2) * K * A + K   # per string: begin + ns write passes + finish; one item reset per batch
+    # per string: begin + one launch per chain pass + finish; one item reset per batch
+    launches = (roofline["passes_per_string"] + 2) * K * A + K
     out = {
         "metric": METRIC, "value": value, "unit": "amps/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": f"c64 arena, f{args.arith} arithmetic", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": 70, "width": w["width"], "strings_per_step": A, "mode": "chain",
-                   "arith": args.arith, "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
+                   "arith": args.arith, "fusion": args.fusion, "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
         "s_per_sample": s_per_sample64, "samples_per_s": world / s_per_sample64,
         "c128": c128, "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
         "clocks": clk.summary(),

@@ -19,6 +19,8 @@
 
 #include "gsb.h"
 #include "gsb_common.h"
+#include "gsb_fuse.h"
+#include "gsb_group.cuh"
 #include "gsb_kernels.cuh"
 #include "gsb_plan.h"
 
@@ -100,10 +102,32 @@ static void *pick_wide(int prec, int ntq, int m, bool write, bool fp32) {
     return m == 2 ? pick_wide128<1, 2>(write) : pick_wide128<1, 1>(write);
 }
 
+template <typename E, typename T>
+static void *pick_group(int d) {
+    return d == 3 ? (void *)k_group<E, T, 3> : (void *)k_group<E, T, 2>;
+}
+
+// One pass of the chain-mode item: a single step (group == false) or a fused group of d steps.
+struct Op {
+    int k0 = 0, d = 1;
+    bool group = false;
+    GroupArgs ga;
+    void *fn = nullptr;
+    int grid = 1;
+    size_t smem = 0;
+    unsigned int ntiles = 0;
+    double entries = 0;       // entries read + written by the pass
+};
+
+constexpr size_t GROUP_SMEM_BUDGET = 96 * 1024;   // two CTAs per SM
+constexpr int GROUP_MIN_R = 12;                   // steps below 2^12 entries run unfused
+
 struct Engine {
     HPlan plan;
     int prec = 64, dev = 0, sms = 0;
     int arith = 32;                      // arithmetic of the complex64 wide-step kernels: 32 (FP32) or 64 (FP64)
+    int fuse_depth = 2;                  // chain mode: largest number of DP steps fused into one pass (1 = none)
+    std::vector<Op> chain_ops;
     size_t esize = 8;
     void *mem = nullptr;
     cudaStream_t stream = nullptr;       // where work is queued (own_stream unless the caller set one)
@@ -214,9 +238,30 @@ struct Engine {
 
     // One item: begin, steps k0..k1-1, finish.  driver decides the passes:
     //   CHAIN: norm + write per step; CHAIN1: write; HYBRID: norm (skipped on device when forced) + write.
+    cudaError_t launch_op(const Op &op, int driver) {
+        if (!op.group) return launch_step(op.k0, true, driver, plan.ns, true, false);
+        Launch L;
+        L.tl = 8;
+        L.cl = op.ga.L;
+        L.nchunks = op.ntiles;
+        Ctx c = ctx(driver, plan.ns, L, true, false);
+        GroupArgs ga = op.ga;
+        void *memp = mem;
+        void *kargs[] = {&ga, &memp, &c};
+        return cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, stream);
+    }
+
     cudaError_t enqueue_item(int driver, bool use_forced, bool use_unif) {
         cudaError_t e = launch_begin();
         if (e != cudaSuccess) return e;
+        if (driver == DRV_CHAIN1 && !chain_ops.empty()) {
+            for (const Op &op : chain_ops) {
+                e = launch_op(op, driver);
+                if (e != cudaSuccess) return e;
+            }
+            k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
+            return cudaGetLastError();
+        }
         for (int k = 0; k < plan.ns; k++) {
             if (driver != DRV_CHAIN1) {
                 e = launch_step(k, false, driver, plan.ns, use_forced, use_unif);
@@ -294,8 +339,118 @@ static int make_args(Engine &E) {
         maxgrid = std::max(maxgrid, (size_t)std::max(E.lw[(size_t)k].grid, E.ln[(size_t)k].grid));
     }
     maxgrid = std::max(maxgrid, (size_t)E.sms * 8);
-    GSB_CK(cudaMalloc(&E.partials, maxgrid * 2 * sizeof(double)));
+    GSB_CK(cudaMalloc(&E.partials, maxgrid * 4 * sizeof(double)));   // up to 3 sums per block (fused groups)
     return 0;
+}
+
+// Group arguments of a fused pass from the host derivation and the steps' descriptors.
+static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
+    const HPlan &p = E.plan;
+    const size_t es = E.esize, vs = (E.prec == 128 || E.arith == 64) ? 16 : 8;
+    (void)es;
+    auto smem_at = [&](int L) {   // intermediate stages only: the first and last step use the arena directly
+        size_t per = 0;
+        for (int s = 1; s < gp.d; s++) per += (size_t)gp.stage_size[s] * vs;
+        return per << L;
+    };
+    int L = gp.L;
+    while (L > 6 && smem_at(L) > GROUP_SMEM_BUDGET) L--;
+    while (L > 8 && smem_at(L) > 48 * 1024) L--;   // prefer more resident CTAs over larger tiles
+    if (smem_at(L) > GROUP_SMEM_BUDGET || L < 6) return false;   // a warp needs 32 class pairs
+    GroupArgs &ga = op.ga;
+    memset(&ga, 0, sizeof ga);
+    ga.d = gp.d;
+    ga.L = L;
+    std::vector<uint64_t> bhi;
+    for (int j = L; j < gp.L; j++) bhi.push_back(1ULL << j);    // low unit vectors beyond the tile
+    bhi.insert(bhi.end(), gp.bhi.begin(), gp.bhi.end());
+    if (bhi.size() > 30) return false;                           // tile index fits 32 bits with room
+    ga.nbhi = (int)bhi.size();
+    for (size_t j = 0; j < bhi.size(); j++) ga.bhi[j] = bhi[j];
+    for (int s = 0; s <= gp.d; s++) ga.ssz[s] = gp.stage_size[s];
+    {
+        const GroupPlan::Step &g0 = gp.step[0], &gd = gp.step[gp.d - 1];
+        const uint64_t mask = (1ULL << L) - 1;
+        for (int j = 0; j < g0.nmem; j++)
+            for (int t = 0; t < g0.ntq; t++) {
+                const uint64_t z = gp.z_in[(size_t)g0.in_idx[j][t]];
+                ga.z0hi[j][t] = z & ~mask;
+                ga.z0lo[j][t] = (uint32_t)(z & mask);
+            }
+        for (int j = 0; j < gd.nmem; j++)
+            for (int tau = 0; tau < gd.m; tau++) {
+                const uint64_t z = gp.z_out[(size_t)gd.out_idx[j][tau]];
+                ga.zdhi[j][tau] = z & ~mask;
+                ga.zdlo[j][tau] = (uint32_t)(z & mask);
+            }
+    }
+    for (int s = 0; s < gp.d; s++) {
+        const HStep &hs = p.st[(size_t)(gp.k0 + s)];
+        const GroupPlan::Step &g = gp.step[s];
+        GroupStepArgs &a = ga.st[s];
+        a.nmem = g.nmem;
+        a.ntq = g.ntq;
+        a.m = g.m;
+        a.k = gp.k0 + s;
+        a.lambda = g.lambda;
+        for (int t = 0; t < g.ntq; t++) {
+            a.tau0[t] = hs.tau0[t];
+            a.tau1[t] = hs.tau1[t];
+            a.par[t] = hs.par[t];
+        }
+        for (int b = 0; b < 2; b++)
+            for (int x = 0; x < 2; x++) { a.Mr[b][x] = hs.Mr[b][x]; a.Mi[b][x] = hs.Mi[b][x]; }
+        for (int j = 0; j < g.nmem; j++) {
+            for (int t = 0; t < g.ntq; t++) a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
+            for (int tau = 0; tau < g.m; tau++) a.out_idx[j][tau] = (unsigned char)g.out_idx[j][tau];
+            a.mpar[j] = (unsigned char)g.mpar[j];
+        }
+    }
+    op.group = true;
+    op.k0 = gp.k0;
+    op.d = gp.d;
+    op.smem = smem_at(L);
+    op.ntiles = 1u << ga.nbhi;
+    if (E.prec == 128) op.fn = pick_group<double2, double>(gp.d);
+    else if (E.arith == 64) op.fn = pick_group<float2, double>(gp.d);
+    else op.fn = pick_group<float2, float>(gp.d);
+    cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET);
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, 256, op.smem) != cudaSuccess || nb < 1) nb = 1;
+    op.grid = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
+    op.entries = gp.entries_moved;
+    return true;
+}
+
+// Chain-mode pass list: wide steps fused greedily into groups of up to fuse_depth steps.
+static void build_chain_ops(Engine &E) {
+    E.chain_ops.clear();
+    const HPlan &p = E.plan;
+    for (int k = 0; k < p.ns;) {
+        const HStep &hs = p.st[(size_t)k];
+        const int r = hs.nk + (hs.tqs.size() == 4 ? 2 : hs.tqs.size() == 2 ? 1 : 0);
+        bool done = false;
+        if (E.fuse_depth >= 2 && r >= GROUP_MIN_R) {
+            for (int d = std::min(E.fuse_depth, FUSE_MAX_STEPS); d >= 2 && !done; d--) {
+                GroupPlan gp;
+                if (!plan_group(p, k, d, 5, 9, gp)) continue;
+                Op op;
+                if (!fill_group(E, gp, op)) continue;
+                E.chain_ops.push_back(op);
+                k += d;
+                done = true;
+            }
+        }
+        if (!done) {
+            Op op;
+            op.k0 = k;
+            op.d = 1;
+            const double r1 = (double)(1ULL << r), r2 = (double)(1ULL << (hs.nk + (hs.m == 2 ? 1 : 0)));
+            op.entries = r1 + r2;
+            E.chain_ops.push_back(op);
+            k++;
+        }
+    }
 }
 
 static int open_plan(const char *text, size_t len, int precision, int device, gsb_engine **out) {
@@ -347,6 +502,7 @@ static int open_plan(const char *text, size_t len, int precision, int device, gs
     if ((e = cudaMemsetAsync(E->d_forced, 0, cap * ns, E->stream)) != cudaSuccess) return cuda_fail(e, "buffers");
     rc = make_args(*E);
     if (rc) { std::string m = g_err; delete E; return fail(rc, m); }
+    build_chain_ops(*E);
     if ((e = cudaStreamSynchronize(E->stream)) != cudaSuccess) return cuda_fail(e, "set-up");
     *out = reinterpret_cast<gsb_engine *>(E);
     return 0;
@@ -779,6 +935,34 @@ int gsb_set_arith(gsb_engine *e, int bits) {
         E->lw[(size_t)k] = E->shape(E->args[(size_t)k], true);
         E->ln[(size_t)k] = E->shape(E->args[(size_t)k], false);
     }
+    build_chain_ops(*E);
+    return 0;
+}
+
+int gsb_set_fusion(gsb_engine *e, int depth) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (depth < 1 || depth > FUSE_MAX_STEPS) return fail(GSB_E_USAGE, "fusion depth must be 1..3");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    E->fuse_depth = depth;
+    for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);
+    E->graphs.clear();
+    build_chain_ops(*E);
+    return 0;
+}
+
+int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries) {
+    if (!e || !group_len) return fail(GSB_E_USAGE, "null argument");
+    const Engine *E = eng(e);
+    for (int k = 0; k < E->plan.ns; k++) {
+        group_len[k] = 0;
+        if (entries) entries[k] = 0;
+    }
+    for (const Op &op : E->chain_ops) {
+        group_len[op.k0] = op.d;
+        if (entries) entries[op.k0] = op.entries;
+    }
     return 0;
 }
 
@@ -799,6 +983,7 @@ int gsb_set_matrices(gsb_engine *e, const double *M) {
     }
     for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);   // the captured graphs hold M by value
     E->graphs.clear();
+    build_chain_ops(*E);
     return 0;
 }
 
@@ -826,6 +1011,26 @@ int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_wri
     k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
     GSB_CK(E->launch_begin());
     GSB_CK(cudaEventRecord(ev[0], E->stream));
+    if (driver == DRV_CHAIN1 && !E->chain_ops.empty()) {   // one timing per pass, reported at its first step
+        std::vector<float> t((size_t)ns, 0.f);
+        for (size_t i = 0; i < E->chain_ops.size(); i++) {
+            GSB_CK(E->launch_op(E->chain_ops[i], driver));
+            GSB_CK(cudaEventRecord(ev[i + 1], E->stream));
+        }
+        k_finish<<<1, 1, 0, E->stream>>>(E->st, E->d_logp, E->d_aux, driver, ns);
+        GSB_CK(cudaStreamSynchronize(E->stream));
+        for (size_t i = 0; i < E->chain_ops.size(); i++) {
+            float a = 0;
+            GSB_CK(cudaEventElapsedTime(&a, ev[i], ev[i + 1]));
+            t[(size_t)E->chain_ops[i].k0] = a;
+        }
+        for (int k = 0; k < ns; k++) {
+            ms_write[k] = t[(size_t)k];
+            if (ms_norm) ms_norm[k] = 0.f;
+        }
+        for (auto &x : ev) cudaEventDestroy(x);
+        return 0;
+    }
     for (int k = 0; k < ns; k++) {
         if (driver == DRV_CHAIN) GSB_CK(E->launch_step(k, false, driver, ns, true, false));
         GSB_CK(cudaEventRecord(ev[(size_t)(2 * k + 1)], E->stream));
@@ -849,7 +1054,7 @@ int gsb_launches_per_item(const gsb_engine *e, int mode, int64_t *launches) {
     if (!e || !launches) return fail(GSB_E_USAGE, "null argument");
     const Engine *E = eng(e);
     const int64_t ns = E->plan.ns;
-    *launches = mode == 0 ? ns + 2 : 2 * ns + 2;
+    *launches = mode == 0 ? (int64_t)E->chain_ops.size() + 2 : 2 * ns + 2;
     return 0;
 }
 

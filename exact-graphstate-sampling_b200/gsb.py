@@ -59,6 +59,8 @@ def _load():
         "gsb_set_stream": (c.c_int, [P, P]),
         "gsb_set_arith": (c.c_int, [P, c.c_int]),
         "gsb_set_matrices": (c.c_int, [P, dp]),
+        "gsb_set_fusion": (c.c_int, [P, c.c_int]),
+        "gsb_fusion_groups": (c.c_int, [P, c.POINTER(c.c_int), dp]),
         "gsb_profile_steps": (c.c_int, [P, i8p, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_launches_per_item": (c.c_int, [P, c.c_int, c.POINTER(c.c_int64)]),
         "gsb_dp_open_text": (c.c_int, [c.c_char_p, c.c_size_t, c.c_int, c.c_int, c.POINTER(P)]),
@@ -83,7 +85,7 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend")
 
@@ -278,6 +280,18 @@ class Engine:
         rows = rows[1:]
         M = np.array([[float(x) for x in r[-8:]] for r in rows], np.float64).reshape(-1)
         _check(_lib.gsb_set_matrices(self.handle, _ptr(np.ascontiguousarray(M), ctypes.c_double)))
+
+    def set_fusion(self, depth):
+        """'chain' mode: fuse up to `depth` consecutive wide steps per pass (1 = no fusion)."""
+        _check(_lib.gsb_set_fusion(self.handle, int(depth)))
+
+    def fusion_groups(self):
+        """(group length per step: the pass starting at step k spans that many steps, 0 inside a pass;
+        table entries read + written by each pass, at its first step)."""
+        g = np.zeros(max(self.ns, 1), np.int32)
+        e = np.zeros(max(self.ns, 1), np.float64)
+        _check(_lib.gsb_fusion_groups(self.handle, _ptr(g, ctypes.c_int), _ptr(e, ctypes.c_double)))
+        return [int(x) for x in g[:self.ns]], e[:self.ns]
 
     def set_arith(self, bits):
         """complex64 wide-step arithmetic: 32 (FP32 sums and rotation, default) or 64 (exact sums + FP64 rotation,

@@ -112,6 +112,13 @@ int gsb_synchronize(gsb_engine *e);
 /* Queue the engine's work on `cuda_stream` (a cudaStream_t of the engine's device; NULL = the engine's own stream),
  * e.g. a framework's current stream, so events recorded there bracket the engine's kernels. */
 int gsb_set_stream(gsb_engine *e, void *cuda_stream);
+/* 'chain' mode fuses runs of up to `depth` consecutive wide steps (tables of >= 2^12 entries) into one pass over
+ * the arena: the intermediate tables of a group live in shared-memory tiles only.  depth 1 disables fusion;
+ * default 2.  Results are those of the unfused steps up to rounding. */
+int gsb_set_fusion(gsb_engine *e, int depth);
+/* Pass structure of 'chain' mode: group_len[k] = number of steps of the pass starting at step k (0 inside a pass);
+ * entries[k] (may be NULL) = table entries the pass reads plus writes. */
+int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries);
 /* Replace every step's rotation matrix: M is [nsteps][2][2] complex (re, im), M[k][b][x] as the plan text lists
  * it.  The layout stays; this is how one engine (one arena) serves all slice plans of make_sliced_plans, which
  * share the layout and differ only in M (sliced_plans.py:1-14). */

@@ -146,3 +146,25 @@ def test_statevector_n24():
     assert np.abs(np.exp2(lp) - ref).max() <= 1e-12
     big = ref > 1e-10                   # log2 amplifies the absolute rounding of very unlikely strings
     assert big.sum() >= 48 and np.abs(lp[big] - np.log2(ref[big])).max() <= 1e-9
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_fused_chain_depths_vs_oracle(wide_case, mode):
+    """'chain' mode with 1, 2 and 3 DP steps fused per pass gives the oracle's log2 Pr and conditionals."""
+    import workloads
+    from oracle import Oracle
+    ns = n = len(wide_case["steps"])
+    strings = workloads.random_strings(ns, 12, seed=41)
+    o = Oracle(wide_case["path"], 128 if mode == "c128" else 64)
+    ref = [o.chain1(s) for s in strings]
+    o.close()
+    with engine(wide_case["path"], mode) as eng:
+        for depth in (1, 2, 3):
+            eng.set_fusion(depth)
+            glen, _ = eng.fusion_groups()
+            assert sum(glen) == ns and (depth == 1 or max(glen) >= 2)
+            lp, cond = eng.chain(strings)
+            for i, (olp, ocond) in enumerate(ref):
+                assert abs(lp[i] - olp) <= lp_tol(mode, olp, n), (depth, i, lp[i], olp)
+                if olp > -n - 3:
+                    assert np.abs(cond[i] - ocond).max() <= cond_tol(mode), depth
