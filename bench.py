@@ -58,6 +58,8 @@ def parse():
     ap.add_argument("--profile-chain", type=int, default=0, metavar="N",
                     help="only evaluate N strings in chain mode on --profile-workload (for ncu captures)")
     ap.add_argument("--profile-workload", default="n70", choices=["n70", "n62"])
+    ap.add_argument("--profile-mode", default="chain", choices=["chain", "sample"],
+                    help="with --profile-chain: evaluate strings (chain) or draw exact samples (sample)")
     ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 128])
     return ap.parse_args()
 
@@ -70,7 +72,10 @@ def profile_chain(args):
     with gsb.Engine.from_text(w["plan"], precision=args.profile_precision) as eng:
         eng.set_arith(args.arith)
         eng.set_fusion(args.fusion)
-        lp, _ = eng.chain(workloads.random_strings(len(w["steps"]), args.profile_chain, seed=9))
+        if args.profile_mode == "sample":
+            _, lp = eng.sample(args.profile_chain, seed=5)
+        else:
+            lp, _ = eng.chain(workloads.random_strings(len(w["steps"]), args.profile_chain, seed=9))
     print(json.dumps({"workload": w["name"], "width": w["width"], "log2p": [float(x) for x in lp]}))
 
 
@@ -308,6 +313,10 @@ def run_gsb(args):
     tpath = os.path.join(ROOT, "profiles", "write_pass_traffic.json")
     if os.path.exists(tpath):
         traffic = json.load(open(tpath)).get("dram_bytes_per_string_c64")
+    # exact-sample passes (look-ahead norm + write per fused pair), per pass
+    sw, sn = eng.profile_steps(strings[0], mode=1)
+    sample_kernel_ms = float(sw.sum() + sn.sum())
+    sample_bytes = float(sum((2 * (1 << st["r"]) + (1 << st["rn"])) for st in steps)) * 8
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic, "peak_kind": peak_kind,
                 "kernel": "chain passes: k_group<float2,float,*> (fused) + k_pair64/k_step (single steps)",
@@ -315,7 +324,9 @@ def run_gsb(args):
                 "fused_passes_frac": (fused_bytes / (fused_ms / 1000.0) / 1e9) / hbm_peak if fused_ms > 0 else None,
                 "unfused_model_bytes_per_string": float(sum(p[0] for p in per)),
                 "unfused_model_GBps": float(sum(p[0] for p in per)) / (kernel_ms / 1000.0) / 1e9,
-                "passes_per_string": int(sum(1 for x in glen if x > 0)), "fusion": args.fusion}
+                "passes_per_string": int(sum(1 for x in glen if x > 0)), "fusion": args.fusion,
+                "sample_kernel_ms": sample_kernel_ms, "sample_norm_ms": float(sn.sum()),
+                "sample_write_ms": float(sw.sum()), "sample_unfused_model_bytes": sample_bytes}
     eng.close()
 
     # complex128 plain form on the first strings of the timed batch, and the c64-vs-c128 agreement

@@ -117,7 +117,15 @@ struct Op {
     size_t smem = 0;
     unsigned int ntiles = 0;
     double entries = 0;       // entries read + written by the pass
+    void *fn_norm = nullptr;  // exact sampling: the pair's look-ahead norm pass
+    int grid_norm = 1;
+    size_t smem_norm = 0;
 };
+
+template <typename E, typename T>
+static void *pick_group_norm() {
+    return (void *)k_group_norm2<E, T>;
+}
 
 constexpr size_t GROUP_SMEM_BUDGET = 96 * 1024;   // two CTAs per SM
 constexpr int GROUP_MIN_R = 12;                   // steps below 2^12 entries run unfused
@@ -127,7 +135,8 @@ struct Engine {
     int prec = 64, dev = 0, sms = 0;
     int arith = 32;                      // arithmetic of the complex64 wide-step kernels: 32 (FP32) or 64 (FP64)
     int fuse_depth = 2;                  // chain mode: largest number of DP steps fused into one pass (1 = none)
-    std::vector<Op> chain_ops;
+    std::vector<Op> chain_ops;           // 'chain' passes
+    std::vector<Op> sample_ops;          // 'prob' / 'sample' passes: pairs with a look-ahead norm pass
     size_t esize = 8;
     void *mem = nullptr;
     cudaStream_t stream = nullptr;       // where work is queued (own_stream unless the caller set one)
@@ -262,6 +271,30 @@ struct Engine {
             k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
             return cudaGetLastError();
         }
+        if (driver == DRV_CHAIN && !sample_ops.empty()) {
+            for (const Op &op : sample_ops) {
+                if (op.group) {
+                    Launch L;
+                    L.tl = 8;
+                    L.cl = op.ga.L;
+                    L.nchunks = op.ntiles;
+                    Ctx c = ctx(driver, plan.ns, L, use_forced, use_unif);
+                    GroupArgs ga = op.ga;
+                    void *memp = mem;
+                    void *kargs[] = {&ga, &memp, &c};
+                    e = cudaLaunchKernel(op.fn_norm, dim3((unsigned)op.grid_norm), dim3(256), kargs, op.smem_norm, stream);
+                    if (e != cudaSuccess) return e;
+                    e = cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, stream);
+                } else {
+                    e = launch_step(op.k0, false, driver, plan.ns, use_forced, use_unif);
+                    if (e != cudaSuccess) return e;
+                    e = launch_step(op.k0, true, driver, plan.ns, use_forced, use_unif);
+                }
+                if (e != cudaSuccess) return e;
+            }
+            k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
+            return cudaGetLastError();
+        }
         for (int k = 0; k < plan.ns; k++) {
             if (driver != DRV_CHAIN1) {
                 e = launch_step(k, false, driver, plan.ns, use_forced, use_unif);
@@ -339,18 +372,18 @@ static int make_args(Engine &E) {
         maxgrid = std::max(maxgrid, (size_t)std::max(E.lw[(size_t)k].grid, E.ln[(size_t)k].grid));
     }
     maxgrid = std::max(maxgrid, (size_t)E.sms * 8);
-    GSB_CK(cudaMalloc(&E.partials, maxgrid * 4 * sizeof(double)));   // up to 3 sums per block (fused groups)
+    GSB_CK(cudaMalloc(&E.partials, maxgrid * 8 * sizeof(double)));   // up to 6 sums per block (fused groups)
     return 0;
 }
 
 // Group arguments of a fused pass from the host derivation and the steps' descriptors.
-static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
+static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, bool sampling = false) {
     const HPlan &p = E.plan;
-    const size_t es = E.esize, vs = (E.prec == 128 || E.arith == 64) ? 16 : 8;
-    (void)es;
+    const size_t vs = (E.prec == 128 || E.arith == 64) ? 16 : 8;
     auto smem_at = [&](int L) {   // intermediate stages only: the first and last step use the arena directly
         size_t per = 0;
         for (int s = 1; s < gp.d; s++) per += (size_t)gp.stage_size[s] * vs;
+        if (sampling) per *= 2;   // the look-ahead pass keeps both branches of the first step
         return per << L;
     };
     int L = gp.L;
@@ -419,11 +452,46 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, 256, op.smem) != cudaSuccess || nb < 1) nb = 1;
     op.grid = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
     op.entries = gp.entries_moved;
+    if (sampling) {
+        op.smem = smem_at(L) / 2;
+        if (E.prec == 128) op.fn_norm = pick_group_norm<double2, double>();
+        else if (E.arith == 64) op.fn_norm = pick_group_norm<float2, double>();
+        else op.fn_norm = pick_group_norm<float2, float>();
+        op.smem_norm = smem_at(L);
+        cudaFuncSetAttribute(op.fn_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET);
+        nb = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn_norm, 256, op.smem_norm) != cudaSuccess || nb < 1) nb = 1;
+        op.grid_norm = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, 256, op.smem) != cudaSuccess || nb < 1) nb = 1;
+        op.grid = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
+    }
     return true;
 }
 
 // Chain-mode pass list: wide steps fused greedily into groups of up to fuse_depth steps.
+static void build_sample_ops(Engine &E) {
+    E.sample_ops.clear();
+    if (E.fuse_depth < 2) return;
+    const HPlan &p = E.plan;
+    for (int k = 0; k < p.ns;) {
+        const HStep &hs = p.st[(size_t)k];
+        const int r = hs.nk + (hs.tqs.size() == 4 ? 2 : hs.tqs.size() == 2 ? 1 : 0);
+        GroupPlan gp;
+        Op op;
+        if (r >= GROUP_MIN_R && plan_group(p, k, 2, 6, 9, gp) && fill_group(E, gp, op, true)) {
+            E.sample_ops.push_back(op);
+            k += 2;
+        } else {
+            Op single;
+            single.k0 = k;
+            E.sample_ops.push_back(single);
+            k++;
+        }
+    }
+}
+
 static void build_chain_ops(Engine &E) {
+    build_sample_ops(E);
     E.chain_ops.clear();
     const HPlan &p = E.plan;
     for (int k = 0; k < p.ns;) {
@@ -1028,6 +1096,49 @@ int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_wri
             ms_write[k] = t[(size_t)k];
             if (ms_norm) ms_norm[k] = 0.f;
         }
+        for (auto &x : ev) cudaEventDestroy(x);
+        return 0;
+    }
+    if (driver == DRV_CHAIN && !E->sample_ops.empty()) {   // per pass: look-ahead norm, then write
+        std::vector<float> tw((size_t)ns, 0.f), tn((size_t)ns, 0.f);
+        std::vector<cudaEvent_t> ev2(2 * E->sample_ops.size() + 1);
+        for (auto &x : ev2) GSB_CK(cudaEventCreate(&x));
+        GSB_CK(cudaEventRecord(ev2[0], E->stream));
+        for (size_t i = 0; i < E->sample_ops.size(); i++) {
+            const Op &op = E->sample_ops[i];
+            if (op.group) {
+                Launch L;
+                L.tl = 8;
+                L.cl = op.ga.L;
+                L.nchunks = op.ntiles;
+                Ctx c = E->ctx(driver, ns, L, true, false);
+                GroupArgs ga = op.ga;
+                void *memp = E->mem;
+                void *kargs[] = {&ga, &memp, &c};
+                GSB_CK(cudaLaunchKernel(op.fn_norm, dim3((unsigned)op.grid_norm), dim3(256), kargs, op.smem_norm, E->stream));
+                GSB_CK(cudaEventRecord(ev2[2 * i + 1], E->stream));
+                GSB_CK(cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, E->stream));
+            } else {
+                GSB_CK(E->launch_step(op.k0, false, driver, ns, true, false));
+                GSB_CK(cudaEventRecord(ev2[2 * i + 1], E->stream));
+                GSB_CK(E->launch_step(op.k0, true, driver, ns, true, false));
+            }
+            GSB_CK(cudaEventRecord(ev2[2 * i + 2], E->stream));
+        }
+        k_finish<<<1, 1, 0, E->stream>>>(E->st, E->d_logp, E->d_aux, driver, ns);
+        GSB_CK(cudaStreamSynchronize(E->stream));
+        for (size_t i = 0; i < E->sample_ops.size(); i++) {
+            float a = 0, b = 0;
+            GSB_CK(cudaEventElapsedTime(&a, ev2[2 * i], ev2[2 * i + 1]));
+            GSB_CK(cudaEventElapsedTime(&b, ev2[2 * i + 1], ev2[2 * i + 2]));
+            tn[(size_t)E->sample_ops[i].k0] = a;
+            tw[(size_t)E->sample_ops[i].k0] = b;
+        }
+        for (int k = 0; k < ns; k++) {
+            ms_write[k] = tw[(size_t)k];
+            if (ms_norm) ms_norm[k] = tn[(size_t)k];
+        }
+        for (auto &x : ev2) cudaEventDestroy(x);
         for (auto &x : ev) cudaEventDestroy(x);
         return 0;
     }

@@ -338,6 +338,180 @@ __device__ __forceinline__ void group_step_any(const GroupArgs &ga, const GroupS
     }
 }
 
+// Branch norms of one step on one tile for both values of the step's bit (the look-ahead of exact sampling): the
+// coset sums are formed once, rotated by both rows of M, the squares of each row's outputs summed into n[b], and, when
+// out[b] is given, the outputs stored to that shared-memory stage buffer.  FIRST reads the stage from the arena.
+template <typename E, typename T, int P, int NTQ, bool FIRST>
+__device__ __forceinline__ void group_step_rows(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
+                                                const uint64_t TB, const int L, typename CplxOf<T>::type *in_buf,
+                                                typename CplxOf<T>::type *out0, typename CplxOf<T>::type *out1,
+                                                const T (&w_r)[2][2], const T (&w_i)[2][2], double &n0, double &n1) {
+    const uint32_t NC = 1u << L;
+    const int LG = P == 2 ? L - 1 : L;
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem, m = gs.m;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    T ns0 = 0, ns1 = 0;
+    for (uint32_t g = g0; g < NG; g += gstride) {
+        const uint32_t pc = (uint32_t)P * g;
+        int pcls[P];
+#pragma unroll
+        for (int c = 0; c < P; c++) pcls[c] = tpar ^ (__popc((pc + c) & (uint32_t)gs.lambda) & 1);
+        for (int j = j0; j < nm; j += jstride) {
+            T S[P][2][2][2];
+#pragma unroll
+            for (int c = 0; c < P; c++)
+#pragma unroll
+                for (int x = 0; x < 2; x++) { S[c][x][0][0] = 0; S[c][x][0][1] = 0; S[c][x][1][0] = 0; S[c][x][1][1] = 0; }
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                T vr[P], vi[P];
+                if (FIRST) {
+                    const uint32_t zl = ga.z0lo[j][t];
+                    const uint64_t a = (TB ^ ga.z0hi[j][t]) | (uint64_t)((pc ^ zl) & ~(uint32_t)(P - 1));
+                    ld_cls<P>(mem, a, P == 2 ? (zl & 1) != 0 : false, vr, vi);
+                } else {
+                    lds_cls<P>(in_buf + (size_t)gs.in_idx[j][t] * NC + pc, vr, vi);
+                }
+                const bool t0 = gs.tau0[t] != 0, t1 = gs.tau1[t] != 0;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    const T sg = ((pcls[c] ^ gs.mpar[j] ^ gs.par[t]) & 1) ? (T)-1 : (T)1;
+                    if (!t0) { S[c][0][0][0] += vr[c]; S[c][0][0][1] += vi[c]; }
+                    else { S[c][0][1][0] += vr[c]; S[c][0][1][1] += vi[c]; }
+                    if (!t1) { S[c][1][0][0] = fmaT(sg, vr[c], S[c][1][0][0]); S[c][1][0][1] = fmaT(sg, vi[c], S[c][1][0][1]); }
+                    else { S[c][1][1][0] = fmaT(sg, vr[c], S[c][1][1][0]); S[c][1][1][1] = fmaT(sg, vi[c], S[c][1][1][1]); }
+                }
+            }
+#pragma unroll
+            for (int b = 0; b < 2; b++) {
+                typename CplxOf<T>::type *out = b ? out1 : out0;
+#pragma unroll
+                for (int tau = 0; tau < 2; tau++) {
+                    if (tau >= m) break;
+                    T orr[P], oi[P];
+#pragma unroll
+                    for (int c = 0; c < P; c++) {
+                        const T xr = S[c][0][tau][0], xi = S[c][0][tau][1], zr = S[c][1][tau][0], zi = S[c][1][tau][1];
+                        T r = w_r[b][0] * xr;
+                        r = fmaT(-w_i[b][0], xi, r);
+                        r = fmaT(w_r[b][1], zr, r);
+                        r = fmaT(-w_i[b][1], zi, r);
+                        T im = w_r[b][0] * xi;
+                        im = fmaT(w_i[b][0], xr, im);
+                        im = fmaT(w_r[b][1], zi, im);
+                        im = fmaT(w_i[b][1], zr, im);
+                        orr[c] = r;
+                        oi[c] = im;
+                        if (b) { ns1 = fmaT(r, r, ns1); ns1 = fmaT(im, im, ns1); }
+                        else { ns0 = fmaT(r, r, ns0); ns0 = fmaT(im, im, ns0); }
+                    }
+                    if (out) sts_cls<P>(out + (size_t)gs.out_idx[j][tau] * NC + pc, orr, oi);
+                }
+            }
+        }
+    }
+    n0 += (double)ns0;
+    n1 += (double)ns1;
+}
+
+template <typename E, typename T, bool FIRST>
+__device__ __forceinline__ void group_step_rows_any(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
+                                                    const uint64_t TB, const int L, typename CplxOf<T>::type *in_buf,
+                                                    typename CplxOf<T>::type *out0, typename CplxOf<T>::type *out1,
+                                                    const T (&w_r)[2][2], const T (&w_i)[2][2], double &n0, double &n1) {
+    constexpr int P = sizeof(E) == 8 ? 2 : 1;
+    switch (gs.ntq) {
+        case 1: group_step_rows<E, T, P, 1, FIRST>(ga, gs, mem, TB, L, in_buf, out0, out1, w_r, w_i, n0, n1); break;
+        case 2: group_step_rows<E, T, P, 2, FIRST>(ga, gs, mem, TB, L, in_buf, out0, out1, w_r, w_i, n0, n1); break;
+        default: group_step_rows<E, T, P, 4, FIRST>(ga, gs, mem, TB, L, in_buf, out0, out1, w_r, w_i, n0, n1); break;
+    }
+}
+
+// Look-ahead norm pass of a pair of steps (k, k+1) for exact sampling ('sample' / 'prob', gsamp2.cpp:39-55): one
+// read-only pass over the table before step k gives n(b) = |L_k(b) T|^2 and n(b, b') = |L_{k+1}(b') L_k(b) T|^2 for
+// every b, b'.  The epilogue draws (or takes) b_k from n(.), then b_{k+1} from n(b_k, .) -- the conditionals of the
+// two-pass chain, since the normalisation between the steps cancels in the ratio -- and leaves both bits and the
+// pair's combined scale 1 / sqrt(n(b_k, b_{k+1})) for the fused write pass.
+template <typename E, typename T>
+__global__ void __launch_bounds__(256) k_group_norm2(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
+    typedef typename CplxOf<T>::type V;
+    DevState *st = cx.st;
+    if (*(volatile int *)&st->dead) return;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int L = ga.L;
+    const uint64_t mask = ((uint64_t)1 << L) - 1;
+    V *b0 = reinterpret_cast<V *>(smem);
+    V *b1 = b0 + ((size_t)ga.ssz[1] << L);
+    T w0r[2][2], w0i[2][2], w1r[2][2], w1i[2][2];
+#pragma unroll
+    for (int b = 0; b < 2; b++)
+#pragma unroll
+        for (int x = 0; x < 2; x++) {
+            w0r[b][x] = (T)ga.st[0].Mr[b][x];
+            w0i[b][x] = (T)ga.st[0].Mi[b][x];
+            w1r[b][x] = (T)ga.st[1].Mr[b][x];
+            w1i[b][x] = (T)ga.st[1].Mi[b][x];
+        }
+    double acc[6] = {0, 0, 0, 0, 0, 0};   // n(0), n(1), n(0,0), n(0,1), n(1,0), n(1,1)
+    unsigned int i0, i1;
+    block_range(cx.nchunks, i0, i1);
+    uint64_t tb = 0;
+    if (i0 < i1) {
+        const uint32_t g = i0 ^ (i0 >> 1);
+        for (int j = 0; j < ga.nbhi; j++)
+            if ((g >> j) & 1) tb ^= ga.bhi[j];
+    }
+    for (unsigned int it = i0; it < i1; it++) {
+        if (it > i0) tb ^= ga.bhi[__ffs((int)it) - 1];
+        const uint64_t TB = tb & ~mask;
+        group_step_rows_any<E, T, true>(ga, ga.st[0], mem, TB, L, nullptr, b0, b1, w0r, w0i, acc[0], acc[1]);
+        __syncthreads();
+        group_step_rows_any<E, T, false>(ga, ga.st[1], mem, TB, L, b0, nullptr, nullptr, w1r, w1i, acc[2], acc[3]);
+        group_step_rows_any<E, T, false>(ga, ga.st[1], mem, TB, L, b1, nullptr, nullptr, w1r, w1i, acc[4], acc[5]);
+        __syncthreads();
+    }
+    double n[6];
+    if (!grid_reduceN<6>(acc, cx, n)) return;
+    // scalar logic of the two steps (gsamp2.cpp:42-49 twice)
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    const int k = ga.st[0].k;
+    const double p1 = n[1] / (n[0] + n[1]);
+    const int bv0 = cx.forced ? cx.forced[row + k] : (cx.unif[row + k] < p1);
+    const double pb0 = bv0 ? p1 : 1 - p1;
+    if (pb0 <= 0) {
+        st->dead = 1;
+        st->logp = -INFINITY;
+        for (int j = k; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
+        return;
+    }
+    st->logp += log2(pb0);
+    cx.bits_out[row + k] = (int8_t)bv0;
+    const double q0 = n[2 + 2 * bv0], q1 = n[3 + 2 * bv0];
+    const double p2 = q1 / (q0 + q1);
+    const int bv1 = cx.forced ? cx.forced[row + k + 1] : (cx.unif[row + k + 1] < p2);
+    const double pb1 = bv1 ? p2 : 1 - p2;
+    if (pb1 <= 0) {
+        st->dead = 1;
+        st->logp = -INFINITY;
+        for (int j = k + 1; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
+        return;
+    }
+    st->logp += log2(pb1);
+    cx.bits_out[row + k + 1] = (int8_t)bv1;
+    st->gbv[0] = bv0;
+    st->gbv[1] = bv1;
+    st->sc = 1.0 / sqrt(bv1 ? q1 : q0);
+}
+
 template <typename E, typename T, int D>
 __global__ void __launch_bounds__(256) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
     typedef typename CplxOf<T>::type V;
@@ -360,7 +534,8 @@ __global__ void __launch_bounds__(256) k_group(const GroupArgs ga, E *__restrict
     T wr[D][2], wi[D][2];
 #pragma unroll
     for (int s = 0; s < D; s++) {
-        const int bv = cx.forced[row + ga.st[s].k];
+        // 'chain' takes the forced bits; the sampling driver takes the bits its look-ahead pass drew
+        const int bv = cx.driver == DRV_CHAIN1 ? cx.forced[row + ga.st[s].k] : st->gbv[s];
         const double f = s == 0 ? st->sc : 1.0;
 #pragma unroll
         for (int x = 0; x < 2; x++) {
@@ -398,7 +573,8 @@ __global__ void __launch_bounds__(256) k_group(const GroupArgs ga, E *__restrict
     }
     double tot[D];
     if (!grid_reduceN<D>(acc, cx, tot)) return;
-    group_chain1_epilogue<D>(cx, ga.st[0].k, tot);
+    if (cx.driver == DRV_CHAIN1) group_chain1_epilogue<D>(cx, ga.st[0].k, tot);
+    else st->prev = tot[D - 1];
 }
 
 }  // namespace gsb

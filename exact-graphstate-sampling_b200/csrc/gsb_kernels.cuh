@@ -54,7 +54,7 @@ struct DevState {
     int dead;         // a zero-probability branch was taken: later passes do nothing
     int item;         // index of the string / sample being evaluated
     unsigned int counter;   // blocks finished in the current launch
-    int pad;
+    int gbv[3];             // bits of a fused group drawn by its look-ahead pass (exact sampling)
 };
 
 struct Ctx {

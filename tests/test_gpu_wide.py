@@ -150,13 +150,15 @@ def test_statevector_n24():
 
 @pytest.mark.parametrize("mode", MODES)
 def test_fused_chain_depths_vs_oracle(wide_case, mode):
-    """'chain' mode with 1, 2 and 3 DP steps fused per pass gives the oracle's log2 Pr and conditionals."""
+    """'chain' mode with 1, 2 and 3 DP steps fused per pass gives the oracle's log2 Pr and conditionals; 'prob' and
+    'sample' (pairs with a look-ahead norm pass) give the oracle's probabilities and bit-identical samples."""
     import workloads
     from oracle import Oracle
     ns = n = len(wide_case["steps"])
     strings = workloads.random_strings(ns, 12, seed=41)
     o = Oracle(wide_case["path"], 128 if mode == "c128" else 64)
     ref = [o.chain1(s) for s in strings]
+    samples_ref = [o.sample(0, 123, i) for i in range(4)]
     o.close()
     with engine(wide_case["path"], mode) as eng:
         for depth in (1, 2, 3):
@@ -168,3 +170,11 @@ def test_fused_chain_depths_vs_oracle(wide_case, mode):
                 assert abs(lp[i] - olp) <= lp_tol(mode, olp, n), (depth, i, lp[i], olp)
                 if olp > -n - 3:
                     assert np.abs(cond[i] - ocond).max() <= cond_tol(mode), depth
+            # 'prob' and 'sample' run pairs of steps with a look-ahead norm pass when fusion is on
+            lpp = eng.prob(strings[:4])
+            for i in range(4):
+                assert abs(lpp[i] - ref[i][0]) <= lp_tol(mode, ref[i][0], n), (depth, i)
+            bits, slp = eng.sample(4, 123)
+            for i in range(4):
+                ob, olp = samples_ref[i]
+                assert list(bits[i]) == list(ob) and abs(slp[i] - olp) <= lp_tol(mode, olp, n), (depth, i)
