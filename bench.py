@@ -57,7 +57,7 @@ def parse():
                     help="'chain' mode: DP steps fused into one pass over the arena (1 = none)")
     ap.add_argument("--profile-chain", type=int, default=0, metavar="N",
                     help="only evaluate N strings in chain mode on --profile-workload (for ncu captures)")
-    ap.add_argument("--profile-workload", default="n70", choices=["n70", "n62"])
+    ap.add_argument("--profile-workload", default="n70", choices=["n70", "n64", "n62"])
     ap.add_argument("--profile-mode", default="chain", choices=["chain", "sample"],
                     help="with --profile-chain: evaluate strings (chain) or draw exact samples (sample)")
     ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 128])
@@ -68,7 +68,9 @@ def profile_chain(args):
     """A bare run for profilers: build the workload, evaluate N strings in chain mode, print nothing else."""
     import gsb
     import workloads
-    w = workloads.matching_n70_w30() if args.profile_workload == "n70" else workloads.matching_instance(62, 62, 3, 13)
+    w = {"n70": workloads.matching_n70_w30,
+         "n64": lambda: workloads.matching_instance(64, 64, 2, 12),     # width 27: a 1.07 GB complex64 arena
+         "n62": lambda: workloads.matching_instance(62, 62, 3, 13)}[args.profile_workload]()
     with gsb.Engine.from_text(w["plan"], precision=args.profile_precision) as eng:
         eng.set_arith(args.arith)
         eng.set_fusion(args.fusion)

@@ -9,6 +9,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -103,32 +104,41 @@ static void *pick_wide(int prec, int ntq, int m, bool write, bool fp32) {
 }
 
 template <typename E, typename T>
-static void *pick_group(int d) {
-    return d == 3 ? (void *)k_group<E, T, 3> : (void *)k_group<E, T, 2>;
+static void *pick_group(int d, int tr) {
+    if (tr) return d == 2 ? (void *)k_group<E, T, 2, 1> : (void *)k_group<E, T, 1, 1>;
+    return d == 3 ? (void *)k_group<E, T, 3, 0> : (void *)k_group<E, T, 2, 0>;
 }
 
-// One pass of the chain-mode item: a single step (group == false) or a fused group of d steps.
+// One pass of an item: a single step (group == false: norm pass + write pass when sampling) or a fused group that
+// writes d steps and, with tr = 1, evaluates the next step's branch norms (sampling only).
 struct Op {
-    int k0 = 0, d = 1;
+    int k0 = 0, d = 1, tr = 0;
     bool group = false;
+    bool norm_first = false;  // sampling: a norm pass of step k0 runs first (its bit has no other source)
     GroupArgs ga;
     void *fn = nullptr;
     int grid = 1;
     size_t smem = 0;
     unsigned int ntiles = 0;
-    double entries = 0;       // entries read + written by the pass
-    void *fn_norm = nullptr;  // exact sampling: the pair's look-ahead norm pass
-    int grid_norm = 1;
-    size_t smem_norm = 0;
+    double entries = 0;       // entries read + written by the pass (the norm pass not included)
 };
 
-template <typename E, typename T>
-static void *pick_group_norm() {
-    return (void *)k_group_norm2<E, T>;
-}
+#ifndef GSB_GROUP_SMEM_PREF
+#define GSB_GROUP_SMEM_PREF (100 * 1024)
+#endif
+#ifndef GSB_GROUP_MAX_L
+#define GSB_GROUP_MAX_L 10
+#endif
+constexpr uint32_t GROUP_SMEM_BUDGET = 200 * 1024;  // shared memory of one fused-pass CTA at most
+constexpr uint32_t GROUP_SMEM_PREF = GSB_GROUP_SMEM_PREF;   // tiles are shrunk to this first (two CTAs per SM)
+constexpr int GROUP_MAX_L = GSB_GROUP_MAX_L;                // at most 2^GROUP_MAX_L classes per tile
+constexpr int GROUP_MIN_R = 12;                     // steps below 2^12 entries run unfused
 
-constexpr size_t GROUP_SMEM_BUDGET = 96 * 1024;   // two CTAs per SM
-constexpr int GROUP_MIN_R = 12;                   // steps below 2^12 entries run unfused
+template <typename E, typename T>
+static uint32_t group_smem_bytes(int D, int TR, const int (&ssz)[4], int L) {
+    if (TR) return D == 2 ? group_smem<E, T, 2, 1>(ssz, L).total : group_smem<E, T, 1, 1>(ssz, L).total;
+    return D == 3 ? group_smem<E, T, 3, 0>(ssz, L).total : group_smem<E, T, 2, 0>(ssz, L).total;
+}
 
 struct Engine {
     HPlan plan;
@@ -136,7 +146,7 @@ struct Engine {
     int arith = 32;                      // arithmetic of the complex64 wide-step kernels: 32 (FP32) or 64 (FP64)
     int fuse_depth = 2;                  // chain mode: largest number of DP steps fused into one pass (1 = none)
     std::vector<Op> chain_ops;           // 'chain' passes
-    std::vector<Op> sample_ops;          // 'prob' / 'sample' passes: pairs with a look-ahead norm pass
+    std::vector<Op> sample_ops;          // 'prob' / 'sample' passes (build_sample_ops)
     size_t esize = 8;
     void *mem = nullptr;
     cudaStream_t stream = nullptr;       // where work is queued (own_stream unless the caller set one)
@@ -247,13 +257,13 @@ struct Engine {
 
     // One item: begin, steps k0..k1-1, finish.  driver decides the passes:
     //   CHAIN: norm + write per step; CHAIN1: write; HYBRID: norm (skipped on device when forced) + write.
-    cudaError_t launch_op(const Op &op, int driver) {
-        if (!op.group) return launch_step(op.k0, true, driver, plan.ns, true, false);
+    cudaError_t launch_op(const Op &op, int driver, bool use_forced = true, bool use_unif = false) {
+        if (!op.group) return launch_step(op.k0, true, driver, plan.ns, use_forced, use_unif);
         Launch L;
         L.tl = 8;
         L.cl = op.ga.L;
         L.nchunks = op.ntiles;
-        Ctx c = ctx(driver, plan.ns, L, true, false);
+        Ctx c = ctx(driver, plan.ns, L, use_forced, use_unif);
         GroupArgs ga = op.ga;
         void *memp = mem;
         void *kargs[] = {&ga, &memp, &c};
@@ -273,23 +283,12 @@ struct Engine {
         }
         if (driver == DRV_CHAIN && !sample_ops.empty()) {
             for (const Op &op : sample_ops) {
-                if (op.group) {
-                    Launch L;
-                    L.tl = 8;
-                    L.cl = op.ga.L;
-                    L.nchunks = op.ntiles;
-                    Ctx c = ctx(driver, plan.ns, L, use_forced, use_unif);
-                    GroupArgs ga = op.ga;
-                    void *memp = mem;
-                    void *kargs[] = {&ga, &memp, &c};
-                    e = cudaLaunchKernel(op.fn_norm, dim3((unsigned)op.grid_norm), dim3(256), kargs, op.smem_norm, stream);
-                    if (e != cudaSuccess) return e;
-                    e = cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, stream);
-                } else {
+                if (!op.group || op.norm_first) {
                     e = launch_step(op.k0, false, driver, plan.ns, use_forced, use_unif);
                     if (e != cudaSuccess) return e;
-                    e = launch_step(op.k0, true, driver, plan.ns, use_forced, use_unif);
                 }
+                e = op.group ? launch_op(op, driver, use_forced, use_unif)
+                             : launch_step(op.k0, true, driver, plan.ns, use_forced, use_unif);
                 if (e != cudaSuccess) return e;
             }
             k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
@@ -376,20 +375,28 @@ static int make_args(Engine &E) {
     return 0;
 }
 
-// Group arguments of a fused pass from the host derivation and the steps' descriptors.
-static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, bool sampling = false) {
+// Whether a step's branch norms are exact functions of M (one coset offset, x = 0 and x = 1 terms in different
+// outputs): n(b) = (|M[b][0]|^2 + |M[b][1]|^2) |T|^2.
+static bool analytic_step(const HStep &hs) {
+    return hs.tqs.size() == 1 && hs.m == 2 && hs.tau1[0] == 1 - hs.tau0[0];
+}
+
+// Group arguments of a fused pass from the host derivation and the steps' descriptors.  The pass writes stage gp.ws;
+// with gp.ws = gp.d - 1 the last step is the trailing norm step.
+static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
     const HPlan &p = E.plan;
-    const size_t vs = (E.prec == 128 || E.arith == 64) ? 16 : 8;
-    auto smem_at = [&](int L) {   // intermediate stages only: the first and last step use the arena directly
-        size_t per = 0;
-        for (int s = 1; s < gp.d; s++) per += (size_t)gp.stage_size[s] * vs;
-        if (sampling) per *= 2;   // the look-ahead pass keeps both branches of the first step
-        return per << L;
+    const int D = gp.ws, TR = gp.d - gp.ws;
+    if (gp.stage_size[0] > 32 || gp.stage_size[D] > 32) return false;
+    // tile size: the largest 2^L classes whose pipeline buffers fit the budget (6 <= L: a warp needs 32 class pairs)
+    auto smem_at = [&](int L) -> uint32_t {
+        const int ssz[4] = {gp.stage_size[0], gp.stage_size[1], gp.stage_size[2], gp.stage_size[3]};
+        if (E.prec == 128) return group_smem_bytes<double2, double>(D, TR, ssz, L);
+        if (E.arith == 64) return group_smem_bytes<float2, double>(D, TR, ssz, L);
+        return group_smem_bytes<float2, float>(D, TR, ssz, L);
     };
-    int L = gp.L;
-    while (L > 6 && smem_at(L) > GROUP_SMEM_BUDGET) L--;
-    while (L > 8 && smem_at(L) > 48 * 1024) L--;   // prefer more resident CTAs over larger tiles
-    if (smem_at(L) > GROUP_SMEM_BUDGET || L < 6) return false;   // a warp needs 32 class pairs
+    int L = std::min(gp.L, GROUP_MAX_L);
+    while (L > 6 && smem_at(L) > GROUP_SMEM_PREF) L--;
+    if (smem_at(L) > GROUP_SMEM_BUDGET || L < 6) return false;
     GroupArgs &ga = op.ga;
     memset(&ga, 0, sizeof ga);
     ga.d = gp.d;
@@ -401,38 +408,68 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, bool sampling = f
     ga.nbhi = (int)bhi.size();
     for (size_t j = 0; j < bhi.size(); j++) ga.bhi[j] = bhi[j];
     for (int s = 0; s <= gp.d; s++) ga.ssz[s] = gp.stage_size[s];
-    {
-        const GroupPlan::Step &g0 = gp.step[0], &gd = gp.step[gp.d - 1];
-        const uint64_t mask = (1ULL << L) - 1;
-        for (int j = 0; j < g0.nmem; j++)
-            for (int t = 0; t < g0.ntq; t++) {
-                const uint64_t z = gp.z_in[(size_t)g0.in_idx[j][t]];
-                ga.z0hi[j][t] = z & ~mask;
-                ga.z0lo[j][t] = (uint32_t)(z & mask);
-            }
-        for (int j = 0; j < gd.nmem; j++)
-            for (int tau = 0; tau < gd.m; tau++) {
-                const uint64_t z = gp.z_out[(size_t)gd.out_idx[j][tau]];
-                ga.zdhi[j][tau] = z & ~mask;
-                ga.zdlo[j][tau] = (uint32_t)(z & mask);
-            }
-    }
+    // Canonical offset order per step (the kernel's compile-time dataflow shapes, GK_*): for m = 2 with every x = 1
+    // term in the other output than its offset's x = 0 term, offsets whose x = 0 term goes to output 0 come first,
+    // and the outputs are relabelled when more than half go to output 1.  Other steps keep their order (GK_ANY).
+    GroupPlan::Step cs[FUSE_MAX_STEPS];
+    int kinds[FUSE_MAX_STEPS], perm[FUSE_MAX_STEPS][4], swp[FUSE_MAX_STEPS];
     for (int s = 0; s < gp.d; s++) {
         const HStep &hs = p.st[(size_t)(gp.k0 + s)];
         const GroupPlan::Step &g = gp.step[s];
+        bool shaped = g.m == 2;
+        int h = 0;
+        for (int t = 0; t < g.ntq; t++) {
+            shaped = shaped && hs.tau1[t] == 1 - hs.tau0[t];
+            h += hs.tau0[t];
+        }
+        swp[s] = shaped && 2 * h > g.ntq;
+        if (swp[s]) h = g.ntq - h;
+        int n = 0;
+        for (int pass = 0; pass < 2; pass++)
+            for (int t = 0; t < g.ntq; t++)
+                if (!shaped ? pass == 0 : ((hs.tau0[t] ^ swp[s]) == pass)) perm[s][n++] = t;
+        kinds[s] = GK_ANY;
+        if (shaped) {
+            if (g.ntq == 1 && h == 0) kinds[s] = GK_1_0;
+            else if (g.ntq == 2) kinds[s] = h == 0 ? GK_2_0 : GK_2_1;
+            else if (g.ntq == 4) kinds[s] = h == 0 ? GK_4_0 : h == 1 ? GK_4_1 : GK_4_2;
+        }
+        cs[s] = g;
+        for (int j = 0; j < g.nmem; j++) {
+            for (int t = 0; t < g.ntq; t++) cs[s].in_idx[j][t] = g.in_idx[j][perm[s][t]];
+            if (swp[s]) std::swap(cs[s].out_idx[j][0], cs[s].out_idx[j][1]);
+        }
+    }
+    {
+        const GroupPlan::Step &g0 = cs[0], &gd = cs[gp.ws - 1];
+        const uint64_t mask = (1ULL << L) - 1;
+        for (size_t i = 0; i < gp.z_in.size(); i++) ga.blk_in[i] = gp.z_in[i] & ~mask;
+        for (size_t i = 0; i < gp.z_out.size(); i++) ga.blk_out[i] = gp.z_out[i] & ~mask;
+        for (int j = 0; j < g0.nmem; j++)
+            for (int t = 0; t < g0.ntq; t++) ga.z0lo[j][t] = (uint32_t)(gp.z_in[(size_t)g0.in_idx[j][t]] & mask);
+        for (int j = 0; j < gd.nmem; j++)
+            for (int tau = 0; tau < gd.m; tau++) ga.zdlo[j][tau] = (uint32_t)(gp.z_out[(size_t)gd.out_idx[j][tau]] & mask);
+    }
+    for (int s = 0; s < gp.d; s++) {
+        const HStep &hs = p.st[(size_t)(gp.k0 + s)];
+        const GroupPlan::Step &g = cs[s];
         GroupStepArgs &a = ga.st[s];
         a.nmem = g.nmem;
         a.ntq = g.ntq;
         a.m = g.m;
         a.k = gp.k0 + s;
+        a.kind = kinds[s];
         a.lambda = g.lambda;
         for (int t = 0; t < g.ntq; t++) {
-            a.tau0[t] = hs.tau0[t];
-            a.tau1[t] = hs.tau1[t];
-            a.par[t] = hs.par[t];
+            a.tau0[t] = hs.tau0[perm[s][t]] ^ swp[s];
+            a.tau1[t] = hs.tau1[perm[s][t]] ^ swp[s];
+            a.par[t] = hs.par[perm[s][t]];
         }
-        for (int b = 0; b < 2; b++)
+        for (int b = 0; b < 2; b++) {
             for (int x = 0; x < 2; x++) { a.Mr[b][x] = hs.Mr[b][x]; a.Mi[b][x] = hs.Mi[b][x]; }
+            a.c[b] = hs.Mr[b][0] * hs.Mr[b][0] + hs.Mi[b][0] * hs.Mi[b][0] + hs.Mr[b][1] * hs.Mr[b][1] +
+                     hs.Mi[b][1] * hs.Mi[b][1];
+        }
         for (int j = 0; j < g.nmem; j++) {
             for (int t = 0; t < g.ntq; t++) a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
             for (int tau = 0; tau < g.m; tau++) a.out_idx[j][tau] = (unsigned char)g.out_idx[j][tau];
@@ -441,55 +478,81 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, bool sampling = f
     }
     op.group = true;
     op.k0 = gp.k0;
-    op.d = gp.d;
+    op.d = gp.ws;
+    op.tr = gp.d - gp.ws;
     op.smem = smem_at(L);
     op.ntiles = 1u << ga.nbhi;
-    if (E.prec == 128) op.fn = pick_group<double2, double>(gp.d);
-    else if (E.arith == 64) op.fn = pick_group<float2, double>(gp.d);
-    else op.fn = pick_group<float2, float>(gp.d);
-    cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET);
+    if (E.prec == 128) op.fn = pick_group<double2, double>(op.d, op.tr);
+    else if (E.arith == 64) op.fn = pick_group<float2, double>(op.d, op.tr);
+    else op.fn = pick_group<float2, float>(op.d, op.tr);
+    if (cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET) != cudaSuccess)
+        return false;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, 256, op.smem) != cudaSuccess || nb < 1) nb = 1;
     op.grid = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
     op.entries = gp.entries_moved;
-    if (sampling) {
-        op.smem = smem_at(L) / 2;
-        if (E.prec == 128) op.fn_norm = pick_group_norm<double2, double>();
-        else if (E.arith == 64) op.fn_norm = pick_group_norm<float2, double>();
-        else op.fn_norm = pick_group_norm<float2, float>();
-        op.smem_norm = smem_at(L);
-        cudaFuncSetAttribute(op.fn_norm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET);
-        nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn_norm, 256, op.smem_norm) != cudaSuccess || nb < 1) nb = 1;
-        op.grid_norm = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, 256, op.smem) != cudaSuccess || nb < 1) nb = 1;
-        op.grid = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
-    }
     return true;
 }
 
-// Chain-mode pass list: wide steps fused greedily into groups of up to fuse_depth steps.
+// Sampling pass list ('prob' / 'sample'): the cheapest cover of the steps, by table entries moved, with
+//   * single steps: norm pass + write pass (read, read, write);
+//   * fused passes of steps k .. k+d-1 (k+1 .. k+d-1 analytic, so their bits need no data), optionally with the
+//     branch norms of step k+d (trailing, tr = 1; at most 3 steps evaluated in one pass).  Step k's bit comes from
+//     the previous pass's trailing norms, from M when step k is analytic, or else from a norm pass launched first.
 static void build_sample_ops(Engine &E) {
     E.sample_ops.clear();
     if (E.fuse_depth < 2) return;
     const HPlan &p = E.plan;
-    for (int k = 0; k < p.ns;) {
-        const HStep &hs = p.st[(size_t)k];
-        const int r = hs.nk + (hs.tqs.size() == 4 ? 2 : hs.tqs.size() == 2 ? 1 : 0);
-        GroupPlan gp;
-        Op op;
-        if (r >= GROUP_MIN_R && plan_group(p, k, 2, 6, 9, gp) && fill_group(E, gp, op, true)) {
-            E.sample_ops.push_back(op);
-            k += 2;
-        } else {
+    const int ns = p.ns;
+    auto rof = [&](int k) { const HStep &h = p.st[(size_t)k]; return h.nk + (h.tqs.size() == 4 ? 2 : h.tqs.size() == 2 ? 1 : 0); };
+    auto size_in = [&](int k) { return k < ns ? std::ldexp(1.0, rof(k)) : 0.0; };
+    auto size_out = [&](int k) { const HStep &h = p.st[(size_t)k]; return std::ldexp(1.0, h.nk + (h.m == 2 ? 1 : 0)); };
+    const double INF = 1e300;
+    // cost[k][t]: entries moved from step k on, t = step k's trailing norms are available
+    std::vector<std::array<double, 2>> cost((size_t)ns + 1, {INF, INF});
+    std::vector<std::array<Op, 2>> best((size_t)ns + 1);
+    cost[(size_t)ns] = {0, 0};
+    for (int k = ns - 1; k >= 0; k--) {
+        const bool an = analytic_step(p.st[(size_t)k]);
+        for (int t = 0; t < 2; t++) {
+            // single step: norm pass + write pass
             Op single;
             single.k0 = k;
-            E.sample_ops.push_back(single);
-            k++;
+            double c = 2 * size_in(k) + size_out(k) + cost[(size_t)k + 1][0];
+            Op pick = single;
+            if (rof(k) >= GROUP_MIN_R) {
+                for (int d = 1; d <= FUSE_MAX_STEPS; d++) {
+                    if (k + d > ns) break;
+                    if (d > 1 && !analytic_step(p.st[(size_t)(k + d - 1)])) break;
+                    for (int tr = 0; tr < 2; tr++) {
+                        if (d + tr < 2 || d + tr > FUSE_MAX_STEPS) continue;
+                        if (tr && (k + d >= ns || analytic_step(p.st[(size_t)(k + d)]))) continue;
+                        const bool nf = !an && !t;
+                        const double cc = (nf ? size_in(k) : 0) + size_in(k) + size_out(k + d - 1) + cost[(size_t)(k + d)][tr];
+                        if (cc >= c) continue;
+                        GroupPlan gp;
+                        Op op;
+                        if (!plan_group(p, k, d + tr, 5, 9, gp, d) || !fill_group(E, gp, op)) continue;
+                        op.norm_first = nf;
+                        op.ga.src = an ? GSRC_ANALYTIC : t ? GSRC_TRAILING : GSRC_NORM;
+                        c = cc;
+                        pick = op;
+                    }
+                }
+            }
+            cost[(size_t)k][(size_t)t] = c;
+            best[(size_t)k][(size_t)t] = pick;
         }
+    }
+    for (int k = 0, t = 0; k < ns;) {
+        const Op &op = best[(size_t)k][(size_t)t];
+        E.sample_ops.push_back(op);
+        t = op.group ? op.tr : 0;
+        k += op.group ? op.d : 1;
     }
 }
 
+// Chain-mode pass list: wide steps fused greedily into groups of up to fuse_depth steps.
 static void build_chain_ops(Engine &E) {
     build_sample_ops(E);
     E.chain_ops.clear();
@@ -671,6 +734,17 @@ static int check_bits(const int8_t *b, int64_t n, int ns, bool allow_free) {
     return 0;
 }
 
+// A fused pass whose tile loads did not complete within its bounded wait sets DevState::err and stops the item;
+// report it (and clear it) after the work has been synchronised.
+static int check_device(Engine *E) {
+    int v = 0;
+    GSB_CK(cudaMemcpy(&v, &E->st->err, sizeof v, cudaMemcpyDeviceToHost));
+    if (!v) return 0;
+    v = 0;
+    GSB_CK(cudaMemcpy(&E->st->err, &v, sizeof v, cudaMemcpyHostToDevice));
+    return fail(GSB_E_CUDA, "a fused pass gave up waiting for its tile loads; results of this call are invalid");
+}
+
 // forced-string batch through graph `kind` (0 chain, 1 prob)
 static int forced_batch(Engine *E, int kind, const int8_t *bits, int64_t nstr, double *log2p, double *cond) {
     const int ns = E->plan.ns;
@@ -682,6 +756,7 @@ static int forced_batch(Engine *E, int kind, const int8_t *bits, int64_t nstr, d
         if (log2p) GSB_CK(cudaMemcpyAsync(log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToHost, E->stream));
         if (cond && ns) GSB_CK(cudaMemcpyAsync(cond + off * ns, E->d_cond, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToHost, E->stream));
         GSB_CK(cudaStreamSynchronize(E->stream));
+        if ((rc = check_device(E))) return rc;
     }
     return 0;
 }
@@ -716,6 +791,7 @@ static int uniform_batch(Engine *E, const double *u, int64_t count, int8_t *bits
         if (log2p) GSB_CK(cudaMemcpyAsync(log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToHost, E->stream));
         if (bits && ns) GSB_CK(cudaMemcpyAsync(bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToHost, E->stream));
         GSB_CK(cudaStreamSynchronize(E->stream));
+        if ((rc = check_device(E))) return rc;
     }
     return 0;
 }
@@ -769,6 +845,7 @@ int gsb_hybrid(gsb_engine *e, const int8_t *forced, int64_t nstr, uint64_t seed,
         if (ns) GSB_CK(cudaMemcpyAsync(bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToHost, E->stream));
         if (cond && ns) GSB_CK(cudaMemcpyAsync(cond + off * ns, E->d_cond, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToHost, E->stream));
         GSB_CK(cudaStreamSynchronize(E->stream));
+        if ((rc = check_device(E))) return rc;
     }
     return 0;
 }
@@ -986,7 +1063,7 @@ int gsb_synchronize(gsb_engine *e) {
     Engine *E = eng(e);
     DevGuard g(E->dev);
     GSB_CK(cudaStreamSynchronize(E->stream));
-    return 0;
+    return check_device(E);
 }
 
 int gsb_set_arith(gsb_engine *e, int bits) {
@@ -1099,30 +1176,17 @@ int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_wri
         for (auto &x : ev) cudaEventDestroy(x);
         return 0;
     }
-    if (driver == DRV_CHAIN && !E->sample_ops.empty()) {   // per pass: look-ahead norm, then write
+    if (driver == DRV_CHAIN && !E->sample_ops.empty()) {   // per pass: its norm pass (if any), then the pass
         std::vector<float> tw((size_t)ns, 0.f), tn((size_t)ns, 0.f);
         std::vector<cudaEvent_t> ev2(2 * E->sample_ops.size() + 1);
         for (auto &x : ev2) GSB_CK(cudaEventCreate(&x));
         GSB_CK(cudaEventRecord(ev2[0], E->stream));
         for (size_t i = 0; i < E->sample_ops.size(); i++) {
             const Op &op = E->sample_ops[i];
-            if (op.group) {
-                Launch L;
-                L.tl = 8;
-                L.cl = op.ga.L;
-                L.nchunks = op.ntiles;
-                Ctx c = E->ctx(driver, ns, L, true, false);
-                GroupArgs ga = op.ga;
-                void *memp = E->mem;
-                void *kargs[] = {&ga, &memp, &c};
-                GSB_CK(cudaLaunchKernel(op.fn_norm, dim3((unsigned)op.grid_norm), dim3(256), kargs, op.smem_norm, E->stream));
-                GSB_CK(cudaEventRecord(ev2[2 * i + 1], E->stream));
-                GSB_CK(cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, E->stream));
-            } else {
-                GSB_CK(E->launch_step(op.k0, false, driver, ns, true, false));
-                GSB_CK(cudaEventRecord(ev2[2 * i + 1], E->stream));
-                GSB_CK(E->launch_step(op.k0, true, driver, ns, true, false));
-            }
+            if (!op.group || op.norm_first) GSB_CK(E->launch_step(op.k0, false, driver, ns, true, false));
+            GSB_CK(cudaEventRecord(ev2[2 * i + 1], E->stream));
+            if (op.group) GSB_CK(E->launch_op(op, driver, true, false));
+            else GSB_CK(E->launch_step(op.k0, true, driver, ns, true, false));
             GSB_CK(cudaEventRecord(ev2[2 * i + 2], E->stream));
         }
         k_finish<<<1, 1, 0, E->stream>>>(E->st, E->d_logp, E->d_aux, driver, ns);

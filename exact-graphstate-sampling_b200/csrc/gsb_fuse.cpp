@@ -62,11 +62,14 @@ uint64_t solve_parity(const std::vector<uint64_t> &v, const std::vector<int> &t)
 
 }  // namespace
 
-bool plan_group(const HPlan &p, int k0, int d, int min_L, int max_L, GroupPlan &gp) {
+bool plan_group(const HPlan &p, int k0, int d, int min_L, int max_L, GroupPlan &gp, int write_stage) {
     if (d < 1 || d > FUSE_MAX_STEPS || k0 < 0 || k0 + d > p.ns) return false;
+    const int ws = write_stage < 0 ? d : write_stage;
+    if (ws < 1 || ws > d) return false;
     gp = GroupPlan();
     gp.k0 = k0;
     gp.d = d;
+    gp.ws = ws;
     std::vector<Sp> T((size_t)d), D((size_t)d);
     for (int s = 0; s < d; s++) {
         const HStep &st = p.st[(size_t)(k0 + s)];
@@ -152,12 +155,12 @@ bool plan_group(const HPlan &p, int k0, int d, int min_L, int max_L, GroupPlan &
         for (int c : seen_out)
             if (c != 1) return false;
     }
-    // in-place safety: (Z_0 + Z_d) n L_0 = Z_0
+    // in-place safety: (Z_0 + Z_ws) n L_0 = Z_0
     Sp L0;
     for (uint64_t a : T[0].basis) L0.add(a);
     for (uint64_t a : D[0].basis) L0.add(a);
     Sp both = Z[0];
-    for (uint64_t z : Z[(size_t)d].basis) both.add(z);
+    for (uint64_t z : Z[(size_t)ws].basis) both.add(z);
     Sp inter;
     for (uint64_t e : both.elements())
         if (L0.contains(e)) inter.add(e);
@@ -188,8 +191,8 @@ bool plan_group(const HPlan &p, int k0, int d, int min_L, int max_L, GroupPlan &
     gp.L = L;
     gp.nb = L + (int)gp.bhi.size();
     gp.z_in = elems[0];
-    gp.z_out = elems[(size_t)d];
-    gp.entries_moved = (double)(gp.stage_size[0] + gp.stage_size[d]) * (double)(1ULL << gp.nb);
+    gp.z_out = elems[(size_t)ws];
+    gp.entries_moved = (double)(gp.stage_size[0] + gp.stage_size[ws]) * (double)(1ULL << gp.nb);
     return true;
 }
 

@@ -33,9 +33,10 @@ struct GroupPlan {
     int L = 0;                          // log2 classes per tile (class-base bits 0..L-1 are address bits 0..L-1)
     int nb = 0;                         // dim B
     std::vector<uint64_t> bhi;          // class-base basis vectors beyond the L low unit vectors (nb - L of them)
+    int ws = 0;                         // stage written to the arena (d, or d - 1 when the last step only feeds norms)
     int stage_size[FUSE_MAX_STEPS + 1] = {0};
     std::vector<uint64_t> z_in;         // elements of Z_0 (stage-0 offsets), index order
-    std::vector<uint64_t> z_out;        // elements of Z_d (stage-d offsets), index order
+    std::vector<uint64_t> z_out;        // elements of Z_ws (offsets of the written stage), index order
     struct Step {
         int nmem = 0, ntq = 0, m = 0;
         uint64_t lambda = 0;
@@ -49,6 +50,8 @@ struct GroupPlan {
 
 // Try to fuse steps k0 .. k0 + d - 1 of a validated plan.  Returns true and fills gp when the group is safe and fits
 // the kernel's limits (stage sizes <= FUSE_MAX_STAGE, at least min_L low unit vectors among the class-base bits).
-bool plan_group(const HPlan &p, int k0, int d, int min_L, int max_L, GroupPlan &gp);
+// write_stage (default d) is the stage the pass stores; with write_stage = d - 1 the last step is evaluated from the
+// stored stage in shared memory only (its branch norms), and safety is checked for the stored stage.
+bool plan_group(const HPlan &p, int k0, int d, int min_L, int max_L, GroupPlan &gp, int write_stage = -1);
 
 }  // namespace gsb

@@ -2,14 +2,13 @@
 //
 // A CTA owns tiles of 2^L classes.  The classes of a tile have bases TB | p (p < 2^L, TB a multiple of 2^L), so for
 // every stage-0 offset z the tile's inputs are one aligned block of 2^L entries at TB ^ (z & ~mask), with class p at
-// position p ^ (z & mask); the same holds for the stage-d outputs.  For each step s of the group, work items
-// (pair of adjacent classes, member j) -- a warp takes 32 consecutive pairs of one member -- read the member's ntq
-// stage-s values (adjacent classes are adjacent entries, so a pair is one 16-byte access for complex64),
-// form the coset's sums with the sign parity(TB & lambda) ^ parity(p & lambda) ^ mpar_j, rotate by M[b_s] (the first
-// step also applies the run's scale), write the m stage-(s+1) values and add their squares to the step's norm.
-// The first step reads the arena directly (each warp access is one contiguous segment: XOR by a constant only
-// permutes lanes inside it), the last step writes the arena directly, and the stages in between stay in shared
-// memory.
+// position p ^ (z & mask); the same holds for the written stage's outputs.  A tile's input blocks are bulk-copied
+// into shared memory (one cp.async.bulk per block, completion on an mbarrier) two tiles ahead of the computation, and
+// the last step stores to the arena directly.  For each step s of the group, work items (pair of
+// adjacent classes, member j) -- a warp takes 32 consecutive pairs of one member -- read the member's ntq stage-s
+// values (adjacent classes are adjacent entries, so a pair is one 16-byte access for complex64), form the coset's
+// sums with the sign parity(TB & lambda) ^ parity(p & lambda) ^ mpar_j, rotate by M[b_s] (the first step also
+// applies the pass's scale), write the m stage-(s+1) values and add their squares to the step's norm.
 // A class's outputs land only in its own input slots or in slots no class reads (checked on the host), so tiles are
 // independent and the pass is race-free in place.
 #pragma once
@@ -18,20 +17,25 @@
 namespace gsb {
 
 struct GroupStepArgs {
-    int nmem, ntq, m, k;
+    int nmem, ntq, m, k, kind;
+    double c[2];              // analytic branch weights |M[b][0]|^2 + |M[b][1]|^2 (one-offset steps)
     int tau0[4], tau1[4], par[4];
     uint64_t lambda;
     double Mr[2][2], Mi[2][2];
     unsigned char in_idx[16][4], out_idx[16][2], mpar[16];
 };
 
+// first-bit source of a sampling pass (group_decide)
+enum { GSRC_ANALYTIC = 0, GSRC_TRAILING = 1, GSRC_NORM = 2 };
+
 struct GroupArgs {
     int d, L, nbhi, ssz[4];
+    int src;               // GSRC_*
     uint64_t bhi[40];
-    uint64_t z0hi[16][4];  // first step: member j, offset t -> stage-0 offset, bits >= L (read from the arena)
-    uint32_t z0lo[16][4];  //                                                 bits <  L
-    uint64_t zdhi[16][2];  // last step: member j, class tau -> stage-d offset, bits >= L (written to the arena)
-    uint32_t zdlo[16][2];
+    uint64_t blk_in[32];   // stage-0 offsets z_i, bits >= L: input block i of a tile is the arena block at TB ^ blk_in[i]
+    uint64_t blk_out[32];  // written-stage offsets, bits >= L: output block i goes to the arena block at TB ^ blk_out[i]
+    uint32_t z0lo[16][4];  // first step: member j, offset t -> bits < L of its stage-0 offset (position p ^ z0lo)
+    uint32_t zdlo[16][2];  // last written step: member j, output tau -> bits < L of its offset
     GroupStepArgs st[3];
 };
 
@@ -123,91 +127,47 @@ __device__ __forceinline__ void group_chain1_epilogue(const Ctx &cx, int k0, con
     st->sc = ldexp(1.0, -st->ek);
 }
 
-// Two complex values of adjacent classes (even p, p ^ 1) at entry index a (a even): the pair is one 16-byte access
-// for a complex64 arena and two for complex128.
-__device__ __forceinline__ void ld_pair(const float2 *m, uint64_t a, float &er, float &ei, float &orr, float &oi) {
-    const float4 v = *reinterpret_cast<const float4 *>(m + a);
-    er = v.x; ei = v.y; orr = v.z; oi = v.w;
-}
-__device__ __forceinline__ void ld_pair(const float2 *m, uint64_t a, double &er, double &ei, double &orr, double &oi) {
-    const float4 v = *reinterpret_cast<const float4 *>(m + a);
-    er = v.x; ei = v.y; orr = v.z; oi = v.w;
-}
-__device__ __forceinline__ void ld_pair(const double2 *m, uint64_t a, double &er, double &ei, double &orr, double &oi) {
-    const double2 u = m[a], v = m[a + 1];
-    er = u.x; ei = u.y; orr = v.x; oi = v.y;
-}
-__device__ __forceinline__ void st_pair(float2 *m, uint64_t a, float er, float ei, float orr, float oi) {
-    *reinterpret_cast<float4 *>(m + a) = make_float4(er, ei, orr, oi);
-}
-__device__ __forceinline__ void st_pair(float2 *m, uint64_t a, double er, double ei, double orr, double oi) {
-    *reinterpret_cast<float4 *>(m + a) = make_float4((float)er, (float)ei, (float)orr, (float)oi);
-}
-__device__ __forceinline__ void st_pair(double2 *m, uint64_t a, double er, double ei, double orr, double oi) {
-    m[a] = make_double2(er, ei);
-    m[a + 1] = make_double2(orr, oi);
-}
-
-// Shared-memory pair access of adjacent classes: one 16-byte access for 8-byte values.
-__device__ __forceinline__ void lds_pair(const float2 *q, float &er, float &ei, float &orr, float &oi) {
-    const float4 v = *reinterpret_cast<const float4 *>(q);
-    er = v.x; ei = v.y; orr = v.z; oi = v.w;
-}
-__device__ __forceinline__ void lds_pair(const double2 *q, double &er, double &ei, double &orr, double &oi) {
-    const double2 u = q[0], v = q[1];
-    er = u.x; ei = u.y; orr = v.x; oi = v.y;
-}
-__device__ __forceinline__ void sts_pair(float2 *q, float er, float ei, float orr, float oi) {
-    *reinterpret_cast<float4 *>(q) = make_float4(er, ei, orr, oi);
-}
-__device__ __forceinline__ void sts_pair(double2 *q, double er, double ei, double orr, double oi) {
-    q[0] = make_double2(er, ei);
-    q[1] = make_double2(orr, oi);
-}
-
-// Arena / shared-memory access of P adjacent classes (even p, then p ^ 1 when P = 2).
+// Permuted access of P adjacent classes (even p, then p + 1 when P = 2): class p + c sits at position pos ^ c of a
+// block (pos = p ^ the offset's low bits), so a pair is two 8-byte accesses (no swap of the halves of one 16-byte
+// access needed) and a complex128 class one 16-byte access.
 template <int P>
-__device__ __forceinline__ void ld_cls(const float2 *m, uint64_t a, bool sw, float (&r)[P], float (&i)[P]) {
-    if (P == 2) {
-        const float4 v = *reinterpret_cast<const float4 *>(m + a);
-        r[0] = sw ? v.z : v.x; i[0] = sw ? v.w : v.y;
-        r[P - 1] = sw ? v.x : v.z; i[P - 1] = sw ? v.y : v.w;
-    } else {
-        const float2 v = m[a + (sw ? 1 : 0)];
-        r[0] = v.x; i[0] = v.y;
-    }
-}
-template <int P>
-__device__ __forceinline__ void ld_cls(const float2 *m, uint64_t a, bool sw, double (&r)[P], double (&i)[P]) {
-    float fr[P], fi[P];
-    ld_cls<P>(m, a, sw, fr, fi);
-#pragma unroll
-    for (int c = 0; c < P; c++) { r[c] = fr[c]; i[c] = fi[c]; }
-}
-template <int P>
-__device__ __forceinline__ void ld_cls(const double2 *m, uint64_t a, bool sw, double (&r)[P], double (&i)[P]) {
+__device__ __forceinline__ void ld_perm(const float2 *m, uint32_t pos, float (&r)[P], float (&i)[P]) {
 #pragma unroll
     for (int c = 0; c < P; c++) {
-        const double2 v = m[a + (uint64_t)((c ^ (sw ? 1 : 0)) & 1)];
+        const float2 v = m[pos ^ (uint32_t)c];
         r[c] = v.x; i[c] = v.y;
     }
 }
 template <int P>
-__device__ __forceinline__ void st_cls(float2 *m, uint64_t a, bool sw, const float (&r)[P], const float (&i)[P]) {
-    if (P == 2) *reinterpret_cast<float4 *>(m + a) = sw ? make_float4(r[P - 1], i[P - 1], r[0], i[0]) : make_float4(r[0], i[0], r[P - 1], i[P - 1]);
-    else m[a + (sw ? 1 : 0)] = make_float2(r[0], i[0]);
+__device__ __forceinline__ void ld_perm(const float2 *m, uint32_t pos, double (&r)[P], double (&i)[P]) {
+#pragma unroll
+    for (int c = 0; c < P; c++) {
+        const float2 v = m[pos ^ (uint32_t)c];
+        r[c] = v.x; i[c] = v.y;
+    }
 }
 template <int P>
-__device__ __forceinline__ void st_cls(float2 *m, uint64_t a, bool sw, const double (&r)[P], const double (&i)[P]) {
-    float fr[P], fi[P];
+__device__ __forceinline__ void ld_perm(const double2 *m, uint32_t pos, double (&r)[P], double (&i)[P]) {
 #pragma unroll
-    for (int c = 0; c < P; c++) { fr[c] = (float)r[c]; fi[c] = (float)i[c]; }
-    st_cls<P>(m, a, sw, fr, fi);
+    for (int c = 0; c < P; c++) {
+        const double2 v = m[pos ^ (uint32_t)c];
+        r[c] = v.x; i[c] = v.y;
+    }
 }
 template <int P>
-__device__ __forceinline__ void st_cls(double2 *m, uint64_t a, bool sw, const double (&r)[P], const double (&i)[P]) {
+__device__ __forceinline__ void st_perm(float2 *m, uint32_t pos, const float (&r)[P], const float (&i)[P]) {
 #pragma unroll
-    for (int c = 0; c < P; c++) m[a + (uint64_t)((c ^ (sw ? 1 : 0)) & 1)] = make_double2(r[c], i[c]);
+    for (int c = 0; c < P; c++) m[pos ^ (uint32_t)c] = make_float2(r[c], i[c]);
+}
+template <int P>
+__device__ __forceinline__ void st_perm(float2 *m, uint32_t pos, const double (&r)[P], const double (&i)[P]) {
+#pragma unroll
+    for (int c = 0; c < P; c++) m[pos ^ (uint32_t)c] = make_float2((float)r[c], (float)i[c]);
+}
+template <int P>
+__device__ __forceinline__ void st_perm(double2 *m, uint32_t pos, const double (&r)[P], const double (&i)[P]) {
+#pragma unroll
+    for (int c = 0; c < P; c++) m[pos ^ (uint32_t)c] = make_double2(r[c], i[c]);
 }
 // shared memory [index][class]: P consecutive values
 template <int P>
@@ -235,22 +195,40 @@ __device__ __forceinline__ void sts_cls(double2 *q, const double (&r)[P], const 
     for (int c = 0; c < P; c++) q[c] = make_double2(r[c], i[c]);
 }
 
+// Shape of a step's coset dataflow inside a group.  The host orders each step's offsets so that the x = 0 terms of
+// the first NTQ - H offsets go to output 0 and those of the last H offsets to output 1, and the x = 1 terms to the
+// other output (relabelling the two outputs where that makes H <= NTQ / 2).  With (NTQ, H) known at compile time
+// the coset sums need no selects; GK_ANY keeps the per-offset output tables (any m, any pattern, ntq <= 4).
+enum { GK_ANY = 0, GK_1_0, GK_2_0, GK_2_1, GK_4_0, GK_4_1, GK_4_2 };
+
 // One step of a group on one tile.  A work item is P adjacent classes (P = 2 for complex64: one 16-byte access) of
 // one member j.  Threads take class groups and, when the tile has fewer class groups than threads, split the members
-// too.  Per coset: the x = 0 terms sum into their output class, the x = 1 terms sum with the sign
-// (-1)^(parity(base & lambda) ^ par_t) into theirs, and each output class is rotated by the M row of the step's bit.
-// FIRST reads the arena, LAST writes it; the other stages use the shared-memory buffers [index][class].
-template <typename E, typename T, int P, int NTQ, bool FIRST, bool LAST>
-__device__ __forceinline__ void group_step(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
-                                           const uint64_t TB, const int L, typename CplxOf<T>::type *in_buf,
-                                           typename CplxOf<T>::type *out_buf, const T (&w_r)[2], const T (&w_i)[2],
-                                           double &acc) {
+// too; a thread walks its members in the outer loop, so the member's tables are read once.
+// Per coset: the x = 0 terms sum into their output, the x = 1 terms sum with the sign (-1)^par_t into theirs, and
+// output tau = M[b][0] * x0-sum + s * M[b][1] * x1-sum with the class sign s = (-1)^(parity(base & lambda) ^ mpar_j)
+// (gsamp2.cpp:32-38 with the sign parity(c & rhoc) ^ par of the reference's term list factored per class).
+// NB input tables (1, or 2 for the look-ahead's two branches of the previous step) are each rotated by NR rows of M
+// (1 for a write pass, 2 for the look-ahead's branch norms); nsum[b][r] gets the squares of table b under row r.
+// FIRST reads the tile's copy of the arena blocks (type E, class p of offset z at [z index][p ^ (z & mask)]), LAST
+// writes the arena (NB = NR = 1; class p of output offset z at TB ^ (z & ~mask) ^ p ^ (z & mask)), the other stages
+// use buffers [value index][class] of type CplxOf<T>; STS stores every (table, row) to such a buffer.  Buffers are
+// byte offsets into the dynamic shared memory.
+template <typename E, typename T, int P, int NTQ, int H, bool FIRST, bool LAST, bool STS, int NB, int NR>
+__device__ __forceinline__ void group_cosets(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
+                                             const uint64_t TB, const int L, const uint32_t (&in)[NB],
+                                             const uint32_t (&out)[NB][NR], const T (&w_r)[NR][2],
+                                             const T (&w_i)[NR][2], T (&nsum)[NB][NR]) {
+    typedef typename CplxOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr bool ANY = H < 0;
     const uint32_t NC = 1u << L;
     const int LG = P == 2 ? L - 1 : L;                 // log2 class groups per tile
     const uint32_t NG = 1u << LG;
     const int tpar = __popcll(TB & gs.lambda) & 1;
-    const int nm = gs.nmem, m = gs.m;
-    // thread -> (first class group, first member, member stride)
+    const int nm = gs.nmem;
+    const int m = ANY ? gs.m : 2;
+    const int ntq = ANY ? gs.ntq : NTQ;
+    const uint32_t lam = (uint32_t)gs.lambda;
     uint32_t g0 = threadIdx.x, gstride = blockDim.x;
     int j0 = 0, jstride = 1;
     if (NG < blockDim.x) {
@@ -259,322 +237,421 @@ __device__ __forceinline__ void group_step(const GroupArgs &ga, const GroupStepA
         j0 = (int)(threadIdx.x >> LG);
         jstride = (int)(blockDim.x >> LG);
     }
-    T nsum = 0;
-    for (uint32_t g = g0; g < NG; g += gstride) {
-        const uint32_t pc = (uint32_t)P * g;
-        int pcls[P];
+    T sgn[NTQ];
+    int ta0[NTQ], ta1[NTQ];
 #pragma unroll
-        for (int c = 0; c < P; c++) pcls[c] = tpar ^ (__popc((pc + c) & (uint32_t)gs.lambda) & 1);
-        for (int j = j0; j < nm; j += jstride) {
-            // sums by (class c, x, tau, re/im); every index below is a compile-time constant (registers)
-            T S[P][2][2][2];
+    for (int t = 0; t < NTQ; t++) {
+        sgn[t] = gs.par[t] ? (T)-1 : (T)1;
+        ta0[t] = ANY ? gs.tau0[t] : (t < NTQ - H ? 0 : 1);
+        ta1[t] = ANY ? gs.tau1[t] : 1 - ta0[t];
+    }
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        // the member's uniform addressing: value indices of its inputs and outputs in their buffers
+        uint32_t zl[NTQ];
+        uint32_t ib[NTQ];
 #pragma unroll
-            for (int c = 0; c < P; c++)
+        for (int t = 0; t < NTQ; t++) {
+            ib[t] = t < ntq ? (uint32_t)gs.in_idx[j][t] * NC : 0u;
+            zl[t] = FIRST && t < ntq ? ga.z0lo[j][t] : 0u;
+        }
+        uint32_t ol[2] = {0, 0}, oidx[2] = {0, 0};
+        E *ob[2] = {mem, mem};
 #pragma unroll
-                for (int x = 0; x < 2; x++) { S[c][x][0][0] = 0; S[c][x][0][1] = 0; S[c][x][1][0] = 0; S[c][x][1][1] = 0; }
+        for (int tau = 0; tau < 2; tau++) {
+            oidx[tau] = tau < m ? (uint32_t)gs.out_idx[j][tau] * NC : 0u;
+            ol[tau] = LAST && tau < m ? ga.zdlo[j][tau] : 0u;
+            if (LAST && tau < m) ob[tau] = mem + (TB ^ ga.blk_out[gs.out_idx[j][tau]]);
+        }
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = (uint32_t)P * g;
+            // x0[b][c][tau][re/im], x1[..]: the coset's x = 0 and signed x = 1 sums per output
+            T x0[NB][P][2][2], x1[NB][P][2][2];
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+#pragma unroll
+                for (int c = 0; c < P; c++)
+#pragma unroll
+                    for (int u = 0; u < 2; u++) { x0[b][c][u][0] = 0; x0[b][c][u][1] = 0; x1[b][c][u][0] = 0; x1[b][c][u][1] = 0; }
 #pragma unroll
             for (int t = 0; t < NTQ; t++) {
-                T vr[P], vi[P];
-                if (FIRST) {
-                    const uint32_t zl = ga.z0lo[j][t];
-                    const uint64_t a = (TB ^ ga.z0hi[j][t]) | (uint64_t)((pc ^ zl) & ~(uint32_t)(P - 1));
-                    ld_cls<P>(mem, a, P == 2 ? (zl & 1) != 0 : false, vr, vi);
-                } else {
-                    lds_cls<P>(in_buf + (size_t)gs.in_idx[j][t] * NC + pc, vr, vi);
-                }
-                const bool t0 = gs.tau0[t] != 0, t1 = gs.tau1[t] != 0;
+                if (t >= ntq) continue;
 #pragma unroll
-                for (int c = 0; c < P; c++) {
-                    const T sg = ((pcls[c] ^ gs.mpar[j] ^ gs.par[t]) & 1) ? (T)-1 : (T)1;
-                    if (!t0) { S[c][0][0][0] += vr[c]; S[c][0][0][1] += vi[c]; }
-                    else { S[c][0][1][0] += vr[c]; S[c][0][1][1] += vi[c]; }
-                    if (!t1) { S[c][1][0][0] = fmaT(sg, vr[c], S[c][1][0][0]); S[c][1][0][1] = fmaT(sg, vi[c], S[c][1][0][1]); }
-                    else { S[c][1][1][0] = fmaT(sg, vr[c], S[c][1][1][0]); S[c][1][1][1] = fmaT(sg, vi[c], S[c][1][1][1]); }
+                for (int b = 0; b < NB; b++) {
+                    T vr[P], vi[P];
+                    if (FIRST) {
+                        ld_perm<P>(reinterpret_cast<const E *>(smem + in[0]) + ib[t], pc ^ zl[t], vr, vi);
+                    } else {
+                        lds_cls<P>(reinterpret_cast<const V *>(smem + in[b]) + (ib[t] + pc), vr, vi);
+                    }
+#pragma unroll
+                    for (int c = 0; c < P; c++) {
+                        if (ANY) {
+                            if (ta0[t]) { x0[b][c][1][0] += vr[c]; x0[b][c][1][1] += vi[c]; }
+                            else { x0[b][c][0][0] += vr[c]; x0[b][c][0][1] += vi[c]; }
+                            if (ta1[t]) { x1[b][c][1][0] = fmaT(sgn[t], vr[c], x1[b][c][1][0]); x1[b][c][1][1] = fmaT(sgn[t], vi[c], x1[b][c][1][1]); }
+                            else { x1[b][c][0][0] = fmaT(sgn[t], vr[c], x1[b][c][0][0]); x1[b][c][0][1] = fmaT(sgn[t], vi[c], x1[b][c][0][1]); }
+                        } else {
+                            x0[b][c][ta0[t]][0] += vr[c];
+                            x0[b][c][ta0[t]][1] += vi[c];
+                            x1[b][c][ta1[t]][0] = fmaT(sgn[t], vr[c], x1[b][c][ta1[t]][0]);
+                            x1[b][c][ta1[t]][1] = fmaT(sgn[t], vi[c], x1[b][c][ta1[t]][1]);
+                        }
+                    }
+                }
+            }
+            // the class sign folds into the x = 1 coefficient
+            T w1r[NR][P], w1i[NR][P];
+#pragma unroll
+            for (int c = 0; c < P; c++) {
+                const bool neg = ((mp ^ __popc((pc + c) & lam)) & 1) != 0;
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    w1r[r][c] = neg ? -w_r[r][1] : w_r[r][1];
+                    w1i[r][c] = neg ? -w_i[r][1] : w_i[r][1];
                 }
             }
 #pragma unroll
             for (int tau = 0; tau < 2; tau++) {
-                if (tau >= m) break;
-                T orr[P], oi[P];
+                if (tau >= m) continue;
+                // outputs that receive no x = 0 (or no x = 1) term skip that product
+                const bool h0 = ANY || (tau == 0 ? NTQ - H > 0 : H > 0);
+                const bool h1 = ANY || (tau == 0 ? H > 0 : NTQ - H > 0);
 #pragma unroll
-                for (int c = 0; c < P; c++) {
-                    const T xr = S[c][0][tau][0], xi = S[c][0][tau][1], zr = S[c][1][tau][0], zi = S[c][1][tau][1];
-                    T r = w_r[0] * xr;
-                    r = fmaT(-w_i[0], xi, r);
-                    r = fmaT(w_r[1], zr, r);
-                    r = fmaT(-w_i[1], zi, r);
-                    T im = w_r[0] * xi;
-                    im = fmaT(w_i[0], xr, im);
-                    im = fmaT(w_r[1], zi, im);
-                    im = fmaT(w_i[1], zr, im);
-                    orr[c] = r;
-                    oi[c] = im;
-                    nsum = fmaT(r, r, nsum);
-                    nsum = fmaT(im, im, nsum);
-                }
-                if (LAST) {
-                    const uint32_t zl = ga.zdlo[j][tau];
-                    const uint64_t a = (TB ^ ga.zdhi[j][tau]) | (uint64_t)((pc ^ zl) & ~(uint32_t)(P - 1));
-                    st_cls<P>(mem, a, P == 2 ? (zl & 1) != 0 : false, orr, oi);
-                } else {
-                    sts_cls<P>(out_buf + (size_t)gs.out_idx[j][tau] * NC + pc, orr, oi);
-                }
-            }
-        }
-    }
-    acc += (double)nsum;
-}
-
-template <typename E, typename T, bool FIRST, bool LAST>
-__device__ __forceinline__ void group_step_any(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
-                                               const uint64_t TB, const int L, typename CplxOf<T>::type *in_buf,
-                                               typename CplxOf<T>::type *out_buf, const T (&w_r)[2],
-                                               const T (&w_i)[2], double &acc) {
-    constexpr int P = sizeof(E) == 8 ? 2 : 1;          // complex64: two classes per 16-byte access
-    switch (gs.ntq) {   // uniform across the grid
-        case 1: group_step<E, T, P, 1, FIRST, LAST>(ga, gs, mem, TB, L, in_buf, out_buf, w_r, w_i, acc); break;
-        case 2: group_step<E, T, P, 2, FIRST, LAST>(ga, gs, mem, TB, L, in_buf, out_buf, w_r, w_i, acc); break;
-        default: group_step<E, T, P, 4, FIRST, LAST>(ga, gs, mem, TB, L, in_buf, out_buf, w_r, w_i, acc); break;
-    }
-}
-
-// Branch norms of one step on one tile for both values of the step's bit (the look-ahead of exact sampling): the
-// coset sums are formed once, rotated by both rows of M, the squares of each row's outputs summed into n[b], and, when
-// out[b] is given, the outputs stored to that shared-memory stage buffer.  FIRST reads the stage from the arena.
-template <typename E, typename T, int P, int NTQ, bool FIRST>
-__device__ __forceinline__ void group_step_rows(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
-                                                const uint64_t TB, const int L, typename CplxOf<T>::type *in_buf,
-                                                typename CplxOf<T>::type *out0, typename CplxOf<T>::type *out1,
-                                                const T (&w_r)[2][2], const T (&w_i)[2][2], double &n0, double &n1) {
-    const uint32_t NC = 1u << L;
-    const int LG = P == 2 ? L - 1 : L;
-    const uint32_t NG = 1u << LG;
-    const int tpar = __popcll(TB & gs.lambda) & 1;
-    const int nm = gs.nmem, m = gs.m;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
-    int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
-        g0 = threadIdx.x & (NG - 1);
-        gstride = NG;
-        j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
-    }
-    T ns0 = 0, ns1 = 0;
-    for (uint32_t g = g0; g < NG; g += gstride) {
-        const uint32_t pc = (uint32_t)P * g;
-        int pcls[P];
+                for (int b = 0; b < NB; b++)
 #pragma unroll
-        for (int c = 0; c < P; c++) pcls[c] = tpar ^ (__popc((pc + c) & (uint32_t)gs.lambda) & 1);
-        for (int j = j0; j < nm; j += jstride) {
-            T S[P][2][2][2];
+                    for (int r = 0; r < NR; r++) {
+                        T orr[P], oii[P];
 #pragma unroll
-            for (int c = 0; c < P; c++)
-#pragma unroll
-                for (int x = 0; x < 2; x++) { S[c][x][0][0] = 0; S[c][x][0][1] = 0; S[c][x][1][0] = 0; S[c][x][1][1] = 0; }
-#pragma unroll
-            for (int t = 0; t < NTQ; t++) {
-                T vr[P], vi[P];
-                if (FIRST) {
-                    const uint32_t zl = ga.z0lo[j][t];
-                    const uint64_t a = (TB ^ ga.z0hi[j][t]) | (uint64_t)((pc ^ zl) & ~(uint32_t)(P - 1));
-                    ld_cls<P>(mem, a, P == 2 ? (zl & 1) != 0 : false, vr, vi);
-                } else {
-                    lds_cls<P>(in_buf + (size_t)gs.in_idx[j][t] * NC + pc, vr, vi);
-                }
-                const bool t0 = gs.tau0[t] != 0, t1 = gs.tau1[t] != 0;
-#pragma unroll
-                for (int c = 0; c < P; c++) {
-                    const T sg = ((pcls[c] ^ gs.mpar[j] ^ gs.par[t]) & 1) ? (T)-1 : (T)1;
-                    if (!t0) { S[c][0][0][0] += vr[c]; S[c][0][0][1] += vi[c]; }
-                    else { S[c][0][1][0] += vr[c]; S[c][0][1][1] += vi[c]; }
-                    if (!t1) { S[c][1][0][0] = fmaT(sg, vr[c], S[c][1][0][0]); S[c][1][0][1] = fmaT(sg, vi[c], S[c][1][0][1]); }
-                    else { S[c][1][1][0] = fmaT(sg, vr[c], S[c][1][1][0]); S[c][1][1][1] = fmaT(sg, vi[c], S[c][1][1][1]); }
-                }
-            }
-#pragma unroll
-            for (int b = 0; b < 2; b++) {
-                typename CplxOf<T>::type *out = b ? out1 : out0;
-#pragma unroll
-                for (int tau = 0; tau < 2; tau++) {
-                    if (tau >= m) break;
-                    T orr[P], oi[P];
-#pragma unroll
-                    for (int c = 0; c < P; c++) {
-                        const T xr = S[c][0][tau][0], xi = S[c][0][tau][1], zr = S[c][1][tau][0], zi = S[c][1][tau][1];
-                        T r = w_r[b][0] * xr;
-                        r = fmaT(-w_i[b][0], xi, r);
-                        r = fmaT(w_r[b][1], zr, r);
-                        r = fmaT(-w_i[b][1], zi, r);
-                        T im = w_r[b][0] * xi;
-                        im = fmaT(w_i[b][0], xr, im);
-                        im = fmaT(w_r[b][1], zi, im);
-                        im = fmaT(w_i[b][1], zr, im);
-                        orr[c] = r;
-                        oi[c] = im;
-                        if (b) { ns1 = fmaT(r, r, ns1); ns1 = fmaT(im, im, ns1); }
-                        else { ns0 = fmaT(r, r, ns0); ns0 = fmaT(im, im, ns0); }
+                        for (int c = 0; c < P; c++) {
+                            const T xr = x0[b][c][tau][0], xi = x0[b][c][tau][1];
+                            const T zr = x1[b][c][tau][0], zi = x1[b][c][tau][1];
+                            T re = 0, im = 0;
+                            if (h0) {
+                                re = w_r[r][0] * xr;
+                                re = fmaT(-w_i[r][0], xi, re);
+                                im = w_r[r][0] * xi;
+                                im = fmaT(w_i[r][0], xr, im);
+                            }
+                            if (h1) {
+                                re = h0 ? fmaT(w1r[r][c], zr, re) : w1r[r][c] * zr;
+                                re = fmaT(-w1i[r][c], zi, re);
+                                im = h0 ? fmaT(w1r[r][c], zi, im) : w1r[r][c] * zi;
+                                im = fmaT(w1i[r][c], zr, im);
+                            }
+                            orr[c] = re;
+                            oii[c] = im;
+                            nsum[b][r] = fmaT(re, re, nsum[b][r]);
+                            nsum[b][r] = fmaT(im, im, nsum[b][r]);
+                        }
+                        if (LAST) st_perm<P>(ob[tau], pc ^ ol[tau], orr, oii);
+                        if (STS) sts_cls<P>(reinterpret_cast<V *>(smem + out[b][r]) + (oidx[tau] + pc), orr, oii);
                     }
-                    if (out) sts_cls<P>(out + (size_t)gs.out_idx[j][tau] * NC + pc, orr, oi);
-                }
             }
         }
     }
-    n0 += (double)ns0;
-    n1 += (double)ns1;
 }
 
-template <typename E, typename T, bool FIRST>
-__device__ __forceinline__ void group_step_rows_any(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
-                                                    const uint64_t TB, const int L, typename CplxOf<T>::type *in_buf,
-                                                    typename CplxOf<T>::type *out0, typename CplxOf<T>::type *out1,
-                                                    const T (&w_r)[2][2], const T (&w_i)[2][2], double &n0, double &n1) {
-    constexpr int P = sizeof(E) == 8 ? 2 : 1;
-    switch (gs.ntq) {
-        case 1: group_step_rows<E, T, P, 1, FIRST>(ga, gs, mem, TB, L, in_buf, out0, out1, w_r, w_i, n0, n1); break;
-        case 2: group_step_rows<E, T, P, 2, FIRST>(ga, gs, mem, TB, L, in_buf, out0, out1, w_r, w_i, n0, n1); break;
-        default: group_step_rows<E, T, P, 4, FIRST>(ga, gs, mem, TB, L, in_buf, out0, out1, w_r, w_i, n0, n1); break;
+template <typename E, typename T, bool FIRST, bool LAST, bool STS, int NB, int NR>
+__device__ __forceinline__ void group_cosets_any(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
+                                                 const uint64_t TB, const int L, const uint32_t (&in)[NB],
+                                                 const uint32_t (&out)[NB][NR], const T (&w_r)[NR][2],
+                                                 const T (&w_i)[NR][2], T (&ns)[NB][NR]) {
+    constexpr int P = sizeof(E) == 8 ? 2 : 1;          // complex64: a thread takes two adjacent classes
+#define GSB_GC(NTQ_, H_) group_cosets<E, T, P, NTQ_, H_, FIRST, LAST, STS, NB, NR>(ga, gs, mem, TB, L, in, out, w_r, w_i, ns)
+    switch (gs.kind) {   // uniform across the grid
+        case GK_1_0: GSB_GC(1, 0); break;
+        case GK_2_0: GSB_GC(2, 0); break;
+        case GK_2_1: GSB_GC(2, 1); break;
+        case GK_4_0: GSB_GC(4, 0); break;
+        case GK_4_1: GSB_GC(4, 1); break;
+        case GK_4_2: GSB_GC(4, 2); break;
+        default: GSB_GC(4, -1); break;
     }
+#undef GSB_GC
 }
 
-// Look-ahead norm pass of a pair of steps (k, k+1) for exact sampling ('sample' / 'prob', gsamp2.cpp:39-55): one
-// read-only pass over the table before step k gives n(b) = |L_k(b) T|^2 and n(b, b') = |L_{k+1}(b') L_k(b) T|^2 for
-// every b, b'.  The epilogue draws (or takes) b_k from n(.), then b_{k+1} from n(b_k, .) -- the conditionals of the
-// two-pass chain, since the normalisation between the steps cancels in the ratio -- and leaves both bits and the
-// pair's combined scale 1 / sqrt(n(b_k, b_{k+1})) for the fused write pass.
-template <typename E, typename T>
-__global__ void __launch_bounds__(256) k_group_norm2(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
+// Bits of a sampling pass ('sample' / 'prob': the normalised two-pass chain, gsamp2.cpp:39-55), decided at the start
+// of the pass.  Step k's branch norms n(b) = |L_k(b) T|^2 come from
+//   GSRC_TRAILING: the previous pass (it evaluated step k on the table it wrote: st->n0, st->n1);
+//   GSRC_NORM:     a norm pass of step k just before this one, which already drew the bit (st->bv, st->sc);
+//   GSRC_ANALYTIC: the step itself: with one coset offset and the x = 0 and x = 1 terms in different outputs, every
+//                  entry v becomes M[b][0] v and +-M[b][1] v, so n(b) = (|M[b][0]|^2 + |M[b][1]|^2) |T|^2 exactly
+//                  (ga.st[s].c[b]; |T|^2 is the stored table's norm for the pass's first step and 1 after it).
+// The group's later steps are always analytic, so one pass writes them all.  Every block computes the same bits
+// from the same inputs; block 0 records them (bits, log2 Pr).  Returns false when the item died here.
+template <int D>
+__device__ __forceinline__ bool group_decide(const GroupArgs &ga, const Ctx &cx, int (&bv)[3], double &scale) {
+    DevState *st = cx.st;
+    const bool rec = blockIdx.x == 0;
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    double lp = 0;
+    scale = 1;
+#pragma unroll
+    for (int s = 0; s < D; s++) {
+        const int k = ga.st[s].k;
+        if (s == 0 && ga.src == GSRC_NORM) {
+            bv[0] = st->bv;
+            scale = st->sc;
+            continue;
+        }
+        double n0, n1;
+        if (s == 0 && ga.src == GSRC_TRAILING) { n0 = st->n0; n1 = st->n1; }
+        else if (s == 0) { n0 = ga.st[0].c[0] * st->prev; n1 = ga.st[0].c[1] * st->prev; }   // |T|^2 as stored
+        else { n0 = ga.st[s].c[0]; n1 = ga.st[s].c[1]; }
+        const double p1 = n1 / (n0 + n1);
+        const int b = cx.forced ? cx.forced[row + k] : (cx.unif[row + k] < p1);
+        const double pb = b ? p1 : 1 - p1;
+        if (!(pb > 0)) {
+            if (rec) {
+                st->dead = 1;
+                st->logp = -INFINITY;
+                for (int j = k; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
+            }
+            return false;
+        }
+        lp += log2(pb);
+        scale /= sqrt(b ? n1 : n0);
+        bv[s] = b;
+        if (rec) cx.bits_out[row + k] = (int8_t)b;
+    }
+    if (rec) st->logp += lp;
+    return true;
+}
+
+// ---------------------------------------------------------------------------------------------------------------
+// Bulk-copy pipeline (sm_90+ PTX: mbarrier transaction counts, cp.async.bulk from global to shared memory).
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// global -> shared, completion counted on the mbarrier (bytes: multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+constexpr long long PIPE_WAIT_CYCLES = 1ll << 31;   // about a second: a tile's loads take microseconds
+
+// Wait for phase `parity` of the mbarrier, at most PIPE_WAIT_CYCLES; gives up early when another thread of the block
+// already gave up (*abort).  Returns false on time-out.
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity, volatile int *abort) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (*abort) return false;
+        if (clock64() - t0 > PIPE_WAIT_CYCLES) return false;
+    }
+    return true;
+}
+
+// Shared-memory layout of a fused pass (bytes; every buffer 16-byte aligned):
+//   [0, 16)  two mbarriers (one per input buffer)
+//   two input tiles   ssz[0] blocks of 2^L arena entries (E), block i = arena block at TB ^ blk_in[i]
+//   stages 1 .. D-1 (and D when a step trails it): [value index][class] (CplxOf<T>)
+struct GroupSmem {
+    uint32_t in0, in_bytes, mid[4], total;
+};
+template <typename E, typename T, int D, int TR>
+__host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L) {
     typedef typename CplxOf<T>::type V;
+    GroupSmem g{};
+    const uint32_t NC = 1u << L;
+    g.in0 = 16;
+    g.in_bytes = (uint32_t)ssz[0] * NC * (uint32_t)sizeof(E);
+    uint32_t off = 16 + 2 * g.in_bytes;
+    for (int s = 1; s <= D - 1 + TR; s++) {
+        g.mid[s] = off;
+        off += (uint32_t)ssz[s] * NC * (uint32_t)sizeof(V);
+    }
+    g.total = off;
+    return g;
+}
+
+// One fused pass: D written steps, then (TR = 1) the branch norms of the next step from the written stage, which
+// stays in shared memory for it.  The bits: 'chain' (CHAIN1) takes the forced bits and the run's power-of-two scale;
+// the sampling driver decides them per block (group_decide).
+// A CTA walks its range of tiles in Gray-code order.  Thread 0 bulk-loads the input blocks of tile n into input
+// buffer n & 1 (completion on that buffer's mbarrier) two tiles ahead: the loads of tile n + 2 are issued as soon as
+// tile n's first step has read its buffer.  The last written step stores straight to the arena.  A tile's writes
+// never reach another class's input (checked on the host), so the early loads are race-free.
+template <typename E, typename T, int D, int TR>
+__global__ void __launch_bounds__(256) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
     DevState *st = cx.st;
     if (*(volatile int *)&st->dead) return;
     extern __shared__ __align__(16) unsigned char smem[];
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
     const int L = ga.L;
+    const uint32_t NC = 1u << L;
     const uint64_t mask = ((uint64_t)1 << L) - 1;
-    V *b0 = reinterpret_cast<V *>(smem);
-    V *b1 = b0 + ((size_t)ga.ssz[1] << L);
-    T w0r[2][2], w0i[2][2], w1r[2][2], w1i[2][2];
+    __shared__ int s_bv[3], s_ok;
+    __shared__ double s_sc;
+    __shared__ volatile int s_abort;
+    if (threadIdx.x == 0) {
+        s_ok = 1;
+        s_abort = 0;
+        if (cx.driver == DRV_CHAIN1) {
+            for (int s = 0; s < D; s++) s_bv[s] = cx.forced[row + ga.st[s].k];
+            s_sc = st->sc;
+        } else {
+            s_ok = group_decide<D>(ga, cx, s_bv, s_sc) ? 1 : 0;
+        }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const GroupSmem sm = group_smem<E, T, D, TR>(ga.ssz, L);
+    const uint32_t bar0 = smem_addr(smem);
+    // per-step M row of the step's bit; the first step carries the pass's scale
+    T w[D][1][2], wj[D][1][2];
+#pragma unroll
+    for (int s = 0; s < D; s++) {
+        const int bv = s_bv[s];
+        const double f = s == 0 ? s_sc : 1.0;
+#pragma unroll
+        for (int x = 0; x < 2; x++) {
+            w[s][0][x] = (T)(f * ga.st[s].Mr[bv][x]);
+            wj[s][0][x] = (T)(f * ga.st[s].Mi[bv][x]);
+        }
+    }
+    T tr_r[2][2], tr_i[2][2];   // trailing step: both rows
 #pragma unroll
     for (int b = 0; b < 2; b++)
 #pragma unroll
         for (int x = 0; x < 2; x++) {
-            w0r[b][x] = (T)ga.st[0].Mr[b][x];
-            w0i[b][x] = (T)ga.st[0].Mi[b][x];
-            w1r[b][x] = (T)ga.st[1].Mr[b][x];
-            w1i[b][x] = (T)ga.st[1].Mi[b][x];
+            tr_r[b][x] = TR ? (T)ga.st[D].Mr[b][x] : (T)0;
+            tr_i[b][x] = TR ? (T)ga.st[D].Mi[b][x] : (T)0;
         }
-    double acc[6] = {0, 0, 0, 0, 0, 0};   // n(0), n(1), n(0,0), n(0,1), n(1,0), n(1,1)
+    constexpr int ND = D + 2 * TR;
+    double acc[ND];
+#pragma unroll
+    for (int s = 0; s < ND; s++) acc[s] = 0;
+    const uint32_t none1[1][1] = {{0}};
+    const uint32_t none2[1][2] = {{0, 0}};
+    const uint32_t m1[1] = {sm.mid[1]}, m1o[1][1] = {{sm.mid[1]}};
+    const uint32_t m2[1] = {sm.mid[2]}, m2o[1][1] = {{sm.mid[2]}};
+    const uint32_t blk_bytes = NC * (uint32_t)sizeof(E);
     unsigned int i0, i1;
     block_range(cx.nchunks, i0, i1);
-    uint64_t tb = 0;
-    if (i0 < i1) {
-        const uint32_t g = i0 ^ (i0 >> 1);
+    // Gray-code tile bases: tile n covers classes gray(n) over bhi (the low L bits are the class index)
+    auto tile_tb = [&](unsigned int n) {
+        const uint32_t g = n ^ (n >> 1);
+        uint64_t t = 0;
         for (int j = 0; j < ga.nbhi; j++)
-            if ((g >> j) & 1) tb ^= ga.bhi[j];
+            if ((g >> j) & 1) t ^= ga.bhi[j];
+        return t & ~mask;
+    };
+    if (threadIdx.x == 0) {
+        mbar_init(bar0, 1);
+        mbar_init(bar0 + 8, 1);
+        mbar_init_fence();
     }
-    for (unsigned int it = i0; it < i1; it++) {
-        if (it > i0) tb ^= ga.bhi[__ffs((int)it) - 1];
-        const uint64_t TB = tb & ~mask;
-        group_step_rows_any<E, T, true>(ga, ga.st[0], mem, TB, L, nullptr, b0, b1, w0r, w0i, acc[0], acc[1]);
-        __syncthreads();
-        group_step_rows_any<E, T, false>(ga, ga.st[1], mem, TB, L, b0, nullptr, nullptr, w1r, w1i, acc[2], acc[3]);
-        group_step_rows_any<E, T, false>(ga, ga.st[1], mem, TB, L, b1, nullptr, nullptr, w1r, w1i, acc[4], acc[5]);
-        __syncthreads();
-    }
-    double n[6];
-    if (!grid_reduceN<6>(acc, cx, n)) return;
-    // scalar logic of the two steps (gsamp2.cpp:42-49 twice)
-    const size_t row = (size_t)st->item * (size_t)cx.ns;
-    const int k = ga.st[0].k;
-    const double p1 = n[1] / (n[0] + n[1]);
-    const int bv0 = cx.forced ? cx.forced[row + k] : (cx.unif[row + k] < p1);
-    const double pb0 = bv0 ? p1 : 1 - p1;
-    if (pb0 <= 0) {
-        st->dead = 1;
-        st->logp = -INFINITY;
-        for (int j = k; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
-        return;
-    }
-    st->logp += log2(pb0);
-    cx.bits_out[row + k] = (int8_t)bv0;
-    const double q0 = n[2 + 2 * bv0], q1 = n[3 + 2 * bv0];
-    const double p2 = q1 / (q0 + q1);
-    const int bv1 = cx.forced ? cx.forced[row + k + 1] : (cx.unif[row + k + 1] < p2);
-    const double pb1 = bv1 ? p2 : 1 - p2;
-    if (pb1 <= 0) {
-        st->dead = 1;
-        st->logp = -INFINITY;
-        for (int j = k + 1; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
-        return;
-    }
-    st->logp += log2(pb1);
-    cx.bits_out[row + k + 1] = (int8_t)bv1;
-    st->gbv[0] = bv0;
-    st->gbv[1] = bv1;
-    st->sc = 1.0 / sqrt(bv1 ? q1 : q0);
-}
-
-template <typename E, typename T, int D>
-__global__ void __launch_bounds__(256) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
-    typedef typename CplxOf<T>::type V;
-    DevState *st = cx.st;
-    if (*(volatile int *)&st->dead) return;
-    const size_t row = (size_t)st->item * (size_t)cx.ns;
-    extern __shared__ __align__(16) unsigned char smem[];
-    const int L = ga.L;
-    const uint64_t mask = ((uint64_t)1 << L) - 1;
-    // intermediate stages 1 .. D-1 in shared memory, [value index][class]
-    V *bufm[3] = {nullptr, nullptr, nullptr};
-    {
-        unsigned char *p = smem;
-        for (int s = 1; s < D; s++) {
-            bufm[s] = reinterpret_cast<V *>(p);
-            p += ((size_t)ga.ssz[s] << L) * sizeof(V);
+    __syncthreads();
+    auto issue_loads = [&](unsigned int n) {   // tile n into buffer (n - i0) & 1
+        const int buf = (int)((n - i0) & 1);
+        const uint32_t bar = bar0 + 8 * (uint32_t)buf;
+        const uint32_t dst = bar0 + sm.in0 + (uint32_t)buf * sm.in_bytes;
+        const uint64_t TBn = tile_tb(n);
+        mbar_arrive_expect_tx(bar, sm.in_bytes);
+        for (int i = 0; i < ga.ssz[0]; i++) bulk_load(dst + (uint32_t)i * blk_bytes, mem + (TBn ^ ga.blk_in[i]), blk_bytes, bar);
+    };
+    int issued = 0;   // tiles whose loads thread 0 issued
+    if (threadIdx.x == 0)
+        for (unsigned int n = i0; n < i1 && n < i0 + 2; n++) {
+            issue_loads(n);
+            issued++;
         }
-    }
-    // per-step M rows of the forced bits (the first step carries the run's scale)
-    T wr[D][2], wi[D][2];
-#pragma unroll
-    for (int s = 0; s < D; s++) {
-        // 'chain' takes the forced bits; the sampling driver takes the bits its look-ahead pass drew
-        const int bv = cx.driver == DRV_CHAIN1 ? cx.forced[row + ga.st[s].k] : st->gbv[s];
-        const double f = s == 0 ? st->sc : 1.0;
-#pragma unroll
-        for (int x = 0; x < 2; x++) {
-            wr[s][x] = (T)(f * ga.st[s].Mr[bv][x]);
-            wi[s][x] = (T)(f * ga.st[s].Mi[bv][x]);
-        }
-    }
-    double acc[D];
-#pragma unroll
-    for (int s = 0; s < D; s++) acc[s] = 0;
-    unsigned int i0, i1;
-    block_range(cx.nchunks, i0, i1);
-    uint64_t tb = 0;
-    if (i0 < i1) {
-        const uint32_t g = i0 ^ (i0 >> 1);
-        for (int j = 0; j < ga.nbhi; j++)
-            if ((g >> j) & 1) tb ^= ga.bhi[j];
-    }
+    int waited = 0;   // tiles whose loads completed
+    bool failed = false;
+    uint64_t tb = i0 < i1 ? tile_tb(i0) : 0;
     for (unsigned int it = i0; it < i1; it++) {
-        if (it > i0) tb ^= ga.bhi[__ffs((int)it) - 1];
-        const uint64_t TB = tb & ~mask;
-        if (D == 2) {
-            group_step_any<E, T, true, false>(ga, ga.st[0], mem, TB, L, nullptr, bufm[1], wr[0], wi[0], acc[0]);
-            __syncthreads();
-            group_step_any<E, T, false, true>(ga, ga.st[1], mem, TB, L, bufm[1], nullptr, wr[1], wi[1], acc[1]);
+        const int buf = (int)((it - i0) & 1);
+        const uint64_t TB = tb;
+        if (!mbar_wait_bounded(bar0 + 8 * (uint32_t)buf, ((it - i0) >> 1) & 1, &s_abort)) s_abort = 1;
+        __syncthreads();
+        if (s_abort) {
+            failed = true;
+            break;
+        }
+        waited++;
+        T ns[D][1][1];
+        T nt[1][2] = {{0, 0}};
+#pragma unroll
+        for (int s = 0; s < D; s++) ns[s][0][0] = 0;
+        const uint32_t tin[1] = {sm.in0 + (uint32_t)buf * sm.in_bytes};
+        // written steps: the first reads the input tile, the last writes the arena (and keeps its stage for the
+        // trailing step); the input buffer is free once the first step is done: tile it + 2 goes there
+        if (D == 1) {
+            group_cosets_any<E, T, true, true, TR == 1, 1, 1>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         } else {
-            group_step_any<E, T, true, false>(ga, ga.st[0], mem, TB, L, nullptr, bufm[1], wr[0], wi[0], acc[0]);
-            __syncthreads();
-            group_step_any<E, T, false, false>(ga, ga.st[1], mem, TB, L, bufm[1], bufm[2], wr[1], wi[1], acc[1]);
-            __syncthreads();
-            group_step_any<E, T, false, true>(ga, ga.st[2], mem, TB, L, bufm[2], nullptr, wr[2], wi[2], acc[2]);
+            group_cosets_any<E, T, true, false, true, 1, 1>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         }
+        if (threadIdx.x == 0 && it + 2 < i1) {
+            issue_loads(it + 2);
+            issued++;
+        }
+        if (D == 2) {
+            group_cosets_any<E, T, false, true, TR == 1, 1, 1>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
+        } else if (D == 3) {
+            group_cosets_any<E, T, false, false, true, 1, 1>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
+            __syncthreads();
+            group_cosets_any<E, T, false, true, false, 1, 1>(ga, ga.st[2], mem, TB, L, m2, none1, w[2], wj[2], ns[2]);
+        }
+        if (TR) {
+            if (D > 1) __syncthreads();
+            const uint32_t(&tmid)[1] = D == 1 ? m1 : m2;
+            group_cosets_any<E, T, false, false, false, 1, 2>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int s = 0; s < D; s++) acc[s] += (double)ns[s][0][0];
+        if (TR) {
+            acc[D] += (double)nt[0][0];
+            acc[ND - 1] += (double)nt[0][1];
+        }
+        if (it + 1 < i1) tb ^= ga.bhi[__ffs((int)(it + 1)) - 1] & ~mask;
     }
-    double tot[D];
-    if (!grid_reduceN<D>(acc, cx, tot)) return;
-    if (cx.driver == DRV_CHAIN1) group_chain1_epilogue<D>(cx, ga.st[0].k, tot);
-    else st->prev = tot[D - 1];
+    if (failed) {
+        // a load never completed: record it, let the loads still in flight land (bounded) and leave the item
+        if (threadIdx.x == 0) {
+            atomicExch(&st->err, 1);
+            st->dead = 1;
+            volatile int never = 0;
+            for (int n = waited; n < issued; n++) mbar_wait_bounded(bar0 + 8 * (uint32_t)(n & 1), (uint32_t)(n >> 1) & 1, &never);
+        }
+        __syncthreads();
+        return;
+    }
+    double tot[ND];
+    if (!grid_reduceN<ND>(acc, cx, tot)) return;
+    if (cx.driver == DRV_CHAIN1) {
+        group_chain1_epilogue<D>(cx, ga.st[0].k, *reinterpret_cast<const double(*)[D]>(tot));
+    } else {
+        st->prev = tot[D - 1];
+        if (TR) {
+            st->n0 = tot[D];
+            st->n1 = tot[ND - 1];
+        }
+    }
 }
 
 }  // namespace gsb

@@ -47,14 +47,14 @@ struct DevState {
     double logscale;  // HYBRID: the reference's running logscale
     double logp;      // running log2 probability
     double sc;        // scale of the next write (CHAIN: 1/sqrt(n_b); CHAIN1: 2^-ek)
-    double n0, n1;    // last norm pass
+    double n0, n1;    // last branch norms of a step (norm pass, or the trailing step of a fused sampling pass)
     double aux;       // resume: log2 Pr(prefix)
     int ek;           // CHAIN1: exponent of the next write's power-of-two scale
     int bv;           // bit of the next write
     int dead;         // a zero-probability branch was taken: later passes do nothing
     int item;         // index of the string / sample being evaluated
     unsigned int counter;   // blocks finished in the current launch
-    int gbv[3];             // bits of a fused group drawn by its look-ahead pass (exact sampling)
+    int err;                // a bounded pipeline wait gave up (reported to the host, cleared when read)
 };
 
 struct Ctx {
