@@ -532,7 +532,7 @@ static void build_sample_ops(Engine &E) {
                         if (cc >= c) continue;
                         GroupPlan gp;
                         Op op;
-                        if (!plan_group(p, k, d + tr, 5, 9, gp, d) || !fill_group(E, gp, op)) continue;
+                        if (!plan_group(p, k, d + tr, 6, GROUP_MAX_L, gp, d) || !fill_group(E, gp, op)) continue;
                         op.norm_first = nf;
                         op.ga.src = an ? GSRC_ANALYTIC : t ? GSRC_TRAILING : GSRC_NORM;
                         c = cc;
@@ -564,7 +564,7 @@ static void build_chain_ops(Engine &E) {
         if (E.fuse_depth >= 2 && r >= GROUP_MIN_R) {
             for (int d = std::min(E.fuse_depth, FUSE_MAX_STEPS); d >= 2 && !done; d--) {
                 GroupPlan gp;
-                if (!plan_group(p, k, d, 5, 9, gp)) continue;
+                if (!plan_group(p, k, d, 6, GROUP_MAX_L, gp)) continue;
                 Op op;
                 if (!fill_group(E, gp, op)) continue;
                 E.chain_ops.push_back(op);
