@@ -11,8 +11,10 @@
 // back to back without host round trips; the slice results accumulate on the device.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -288,13 +290,10 @@ int gsb_dp_run(gsb_dp *d, int64_t nslices, const double *pre, const double *w, d
     return 0;
 }
 
-// One out-of-place step on a caller table (complex128, host memory): the reference's sampler_ref.extend
-// (sampler_ref.py:8-23) and ref.run's inner step (ref.py:18-31).
-int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker, const double *wv,
-                  const double *old, double *out, int device) {
-    if (r < 0 || rn < 0 || r > 30 || rn > 30 || nker < 0 || nker > 2 || (nker && !ker) || !wv || !old || !out)
-        return dp_fail(GSB_E_USAGE, "bad argument");
-    DpStep st;
+}  // extern "C"
+
+// Step descriptor of gsb_dp_extend / gsb_dp_extend_static from the caller's arguments (arguments already checked).
+static int extend_step(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker, DpStep &st) {
     memset(&st, 0, sizeof st);
     st.v = 0;
     st.r = r;
@@ -313,6 +312,43 @@ int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const
             st.pos[st.npos++] = (uint64_t)b;
         }
     if (st.npos != rn) return dp_fail(GSB_E_USAGE, "pivot mask must have rn bits");
+    return 0;
+}
+
+// Scratch of gsb_dp_extend_static, in the library's static device memory (every GPU that loads the library holds it
+// until the process exits): the old table, the new table (2^EXTEND_STATIC_LOG2 complex128 entries each) and the
+// weights.  Calls share it; each call overwrites what it uses (the kernel writes every entry of the new table, so
+// nothing has to start at zero).
+constexpr int EXTEND_STATIC_LOG2 = 16;
+constexpr size_t EXTEND_STATIC_N = (size_t)1 << EXTEND_STATIC_LOG2;
+static __device__ __align__(256) double2 g_extend_scratch[2 * EXTEND_STATIC_N + 2];   // 2 MiB + 32 B
+
+// Device address of the scratch on `device` (current), looked up once per device and kept.
+static int extend_scratch(int device, double2 **out) {
+    static std::mutex mu;
+    static std::vector<double2 *> addr;
+    std::lock_guard<std::mutex> lock(mu);
+    if ((size_t)device >= addr.size()) addr.resize((size_t)device + 1, nullptr);
+    if (!addr[(size_t)device]) {
+        void *p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_extend_scratch);
+        if (e != cudaSuccess) return dp_fail(GSB_E_CUDA, std::string("static scratch lookup: ") + cudaGetErrorString(e));
+        addr[(size_t)device] = static_cast<double2 *>(p);
+    }
+    *out = addr[(size_t)device];
+    return 0;
+}
+
+extern "C" {
+
+// One out-of-place step on a caller table (complex128, host memory): the reference's sampler_ref.extend
+// (sampler_ref.py:8-23) and ref.run's inner step (ref.py:18-31).
+int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker, const double *wv,
+                  const double *old, double *out, int device) {
+    if (r < 0 || rn < 0 || r > 30 || rn > 30 || nker < 0 || nker > 2 || (nker && !ker) || !wv || !old || !out)
+        return dp_fail(GSB_E_USAGE, "bad argument");
+    DpStep st;
+    if (int rc = extend_step(r, rn, rho, pivmask, nker, ker, st)) return rc;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(device);
@@ -335,6 +371,37 @@ int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const
     cudaFree(b);
     cudaFree(w);
     DP_CK(e);
+    return 0;
+}
+
+// gsb_dp_extend without any device allocation: the tables and weights go through the static scratch above, so
+// r and rn are limited to EXTEND_STATIC_LOG2.  The first call on a device looks up the scratch's address.
+int gsb_dp_extend_static(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker,
+                         const double *wv, const double *old, double *out, int device) {
+    if (r < 0 || rn < 0 || nker < 0 || nker > 2 || (nker && !ker) || !wv || !old || !out)
+        return dp_fail(GSB_E_USAGE, "bad argument");
+    if (r > EXTEND_STATIC_LOG2 || rn > EXTEND_STATIC_LOG2)
+        return dp_fail(GSB_E_USAGE, "table too large for the static scratch: r and rn must be at most " +
+                                        std::to_string(EXTEND_STATIC_LOG2));
+    DpStep st;
+    if (int rc = extend_step(r, rn, rho, pivmask, nker, ker, st)) return rc;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    DP_CK(cudaSetDevice(device));
+    struct Restore {
+        int p;
+        ~Restore() { cudaSetDevice(p); }
+    } restore{prev};
+    double2 *scratch = nullptr;
+    if (int rc = extend_scratch(device, &scratch)) return rc;
+    double2 *a = scratch, *b = scratch + EXTEND_STATIC_N;
+    double *w = reinterpret_cast<double *>(scratch + 2 * EXTEND_STATIC_N);
+    const size_t na = (size_t)1 << r, nb = (size_t)1 << rn;
+    DP_CK(cudaMemcpy(a, old, na * 16, cudaMemcpyHostToDevice));
+    DP_CK(cudaMemcpy(w, wv, 32, cudaMemcpyHostToDevice));
+    k_dp_step<double2><<<(unsigned)std::min<size_t>((nb + 255) / 256, 4096), 256>>>(st, a, b, w);
+    DP_CK(cudaGetLastError());
+    DP_CK(cudaMemcpy(out, b, nb * 16, cudaMemcpyDeviceToHost));
     return 0;
 }
 

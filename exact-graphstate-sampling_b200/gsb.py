@@ -68,6 +68,8 @@ def _load():
         "gsb_dp_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_dp_run": (c.c_int, [P, c.c_int64, dp, dp, dp]),
         "gsb_dp_extend": (c.c_int, [c.c_int, c.c_int, c.c_uint64, c.c_uint64, c.c_int, u64p, dp, dp, dp, c.c_int]),
+        "gsb_dp_extend_static": (c.c_int, [c.c_int, c.c_int, c.c_uint64, c.c_uint64, c.c_int, u64p, dp, dp, dp,
+                                           c.c_int]),
         "gsb_validate_text": (c.c_int, [c.c_char_p, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
                                         c.POINTER(c.c_int)]),
         "gsb_cut_profile": (c.c_int, [c.c_int, c.POINTER(c.c_uint8), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
@@ -87,7 +89,7 @@ EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "g
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
            "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
-           "gsb_dp_extend")
+           "gsb_dp_extend", "gsb_dp_extend_static")
 
 
 def lib():
@@ -360,18 +362,26 @@ class DpEngine:
             pass
 
 
-def dp_extend(old, r, rn, rho, piv, ker, wv, device=0):
-    """One out-of-place DP step on the GPU (complex128): new table of 2^rn entries."""
+def _extend(fn, old, r, rn, rho, piv, ker, wv, device):
     old = np.ascontiguousarray(old, np.complex128)
     assert old.shape == (1 << r,)
     out = np.zeros(1 << rn, np.complex128)
     k = np.ascontiguousarray(list(ker) or [0], np.uint64)
     w = np.array([complex(wv[0]).real, complex(wv[0]).imag, complex(wv[1]).real, complex(wv[1]).imag])
     pm = sum(1 << p for p in piv)
-    _check(_lib.gsb_dp_extend(int(r), int(rn), int(rho), int(pm), len(ker), _ptr(k, ctypes.c_uint64),
-                              _ptr(w, ctypes.c_double), _ptr(old.view(np.float64), ctypes.c_double),
-                              _ptr(out.view(np.float64), ctypes.c_double), int(device)))
+    _check(fn(int(r), int(rn), int(rho), int(pm), len(ker), _ptr(k, ctypes.c_uint64), _ptr(w, ctypes.c_double),
+              _ptr(old.view(np.float64), ctypes.c_double), _ptr(out.view(np.float64), ctypes.c_double), int(device)))
     return out
+
+
+def dp_extend(old, r, rn, rho, piv, ker, wv, device=0):
+    """One out-of-place DP step on the GPU (complex128): new table of 2^rn entries."""
+    return _extend(_lib.gsb_dp_extend, old, r, rn, rho, piv, ker, wv, device)
+
+
+def dp_extend_static(old, r, rn, rho, piv, ker, wv, device=0):
+    """dp_extend without device allocation (static scratch in the library; r, rn <= 16; calls must not overlap)."""
+    return _extend(_lib.gsb_dp_extend_static, old, r, rn, rho, piv, ker, wv, device)
 
 
 def validate_text(text):

@@ -151,6 +151,16 @@ int gsb_dp_run(gsb_dp *d, int64_t nslices, const double *pre, const double *w, d
  * wv = (w0 re, w0 im, w1 re, w1 im) (sampler_ref.py:8-23 `extend`, ref.py:18-31). */
 int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker, const double *wv,
                   const double *old_table, double *new_table, int device);
+/* gsb_dp_extend for callers that cannot allocate device memory (no counterpart in the reference): it calls no
+ * cudaMalloc / cudaFree (which synchronise the device, and fail when another allocator, e.g. a framework's caching
+ * allocator, already holds the free HBM).  The old table, the new table and the weights go through a static
+ * scratch array in the library's device memory, 2 MiB + 32 B per GPU that loads the library, held until the process
+ * exits, so r and rn must be at most 16 (larger tables return GSB_E_USAGE).  The first call on a device looks up the
+ * scratch's address (cudaGetSymbolAddress); make that first call before any stream capture.  All calls share the
+ * scratch: calls that overlap in time on one device (from several host threads) race and must be serialised by the
+ * caller. */
+int gsb_dp_extend_static(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker,
+                         const double *wv, const double *old_table, double *new_table, int device);
 
 /* ---- host-side helpers (no GPU needed) ---- */
 
