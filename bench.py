@@ -35,6 +35,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 PKG = os.path.join(ROOT, "exact-graphstate-sampling_b200")
 sys.path.insert(0, PKG)
 sys.path.insert(0, ROOT)
+import replicas  # noqa: E402  (package module: torchrun rank bookkeeping)
 
 METRIC = "s/sample & amps/s at n=70 w=30, c64 form vs c128 plain, |Δlog2P|≤1e-5; HBM GB/s"
 WORKLOAD = "matching_n70_d70_s2_w30"
@@ -137,33 +138,6 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_init(n):
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    return rank, world, local
-
-
-def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
-
-
 def ref_chain_time(plan_path, strings_path, threads):
     """Wall time of the reference executor ('chain' mode, complex64) on the strings file, and its stdout."""
     from oracle import ref_binary, run_ref
@@ -184,8 +158,7 @@ def ref_chain_time(plan_path, strings_path, threads):
 
 
 def run_reference(args):
-    rank, world, local = dist_init(args.gpus)
-    if rank != 0:
+    if int(os.environ.get("RANK", "0")) != 0:   # rank 0 alone times the host reference; no process group needed
         return
     import workloads
     w = workloads.matching_n70_w30()
@@ -220,7 +193,7 @@ def run_reference(args):
 def run_gsb(args):
     import numpy as np
     import torch
-    rank, world, local = dist_init(args.gpus)
+    rank, world, local = replicas.init()
     torch.cuda.set_device(local)
     import gsb
     import workloads
@@ -248,7 +221,7 @@ def run_gsb(args):
     for i in range(W):
         amp_step(i)
     torch.cuda.synchronize()
-    barrier(world)
+    replicas.barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with Clocks(local) as clk:
@@ -257,10 +230,10 @@ def run_gsb(args):
             amp_step(i)
         ev1.record(stream)
         torch.cuda.synchronize()
-    barrier(world)
+    replicas.barrier(world)
     torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms, world)
+    ms_max = replicas.max_over_ranks(ms, world)
     value = world * K * A / (ms_max / 1000.0)
     lp64 = d_lp.cpu().numpy()
     cond64 = d_cond.cpu().numpy()
@@ -270,11 +243,11 @@ def run_gsb(args):
     host = pinned.numpy()
     eng.chain(host[:A])
     torch.cuda.synchronize()
-    barrier(world)
+    replicas.barrier(world)
     t0 = time.perf_counter()
     for i in range(K):
         eng.chain(host[i * A:(i + 1) * A])
-    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_s = replicas.max_over_ranks(time.perf_counter() - t0, world)
     e2e = {"value": world * K * A / e2e_s, "unit": "amps/s", "h2d_bytes_per_step": A * ns,
            "d2h_bytes_per_step": A * 8 + A * ns * 8}
 
@@ -291,7 +264,7 @@ def run_gsb(args):
     eng.sample_device(d_u, d_sb, d_slp)
     e1.record(stream)
     torch.cuda.synchronize()
-    s_per_sample64 = max_over_ranks(e0.elapsed_time(e1) / 1000.0 / S, world)
+    s_per_sample64 = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0 / S, world)
     sbits64 = d_sb.cpu().numpy()
 
     # roofline of the dominant kernels (the chain-mode passes: fused groups k_group and single steps), timed per
@@ -359,7 +332,7 @@ def run_gsb(args):
         s_per_sample128 = e0.elapsed_time(e1) / 1000.0 / S2
         same_bits = bool((d_sb[:S2].cpu().numpy() == sbits64[:S2]).all())
         e128.close()
-        c128 = {"amps_per_s": max_over_ranks(amps128, world) if world == 1 else amps128,
+        c128 = {"amps_per_s": amps128,
                 "s_per_sample": s_per_sample128, "max_abs_dlog2p_c64_vs_c128": dlp,
                 "max_abs_dcond_c64_vs_c128": dcond, "samples_same_bits_c64_c128": same_bits}
 
@@ -389,9 +362,7 @@ def run_gsb(args):
                                    "abs_dlog2p_vs_gpu_c64": abs(ref_lp - float(lp64[W * A]))}
     if rank == 0:
         print(json.dumps(out), flush=True)
-    if world > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    replicas.finish(world)
 
 
 if __name__ == "__main__":
