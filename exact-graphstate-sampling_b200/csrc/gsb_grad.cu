@@ -1,0 +1,406 @@
+// Adjoint sweep of the in-place cut-rank DP (complex128): gradients of log Pr(b) with respect to the step matrices.
+//
+// The forward sweep of a string b is linear in every table and in every step's M row:
+//   T_{k+1} = L_k(M_k[b_k]) T_k,   Z(b) = T_ns[0],   Pr(b) = 2^-n |Z(b)|^2,
+// with the step map of the executor (gsamp2.cpp:32-38, 59-66): for every coset c of step k, base = XOR of Tkeep
+// over the bits of c, the inputs v_t = T_k[base ^ tq_t] and
+//   out[tau] = sum_{t: tau0_t = tau} m0 v_t + sum_{t: tau1_t = tau} m1 s_t v_t,   s_t = (-1)^(parity(c & rhoc) ^ par_t),
+// m_x = M_k[b_k][x], stored at base (tau 0) and base ^ g (tau 1).  The reverse sweep carries lambda_k = dZ/dT_k
+// backwards through the transposed step map (the same cosets and slots, read and written the other way round):
+//   lambda_k[base ^ tq_t] = m0 lambda_{k+1}[tau0_t] + m1 s_t lambda_{k+1}[tau1_t],
+//   dZ/dm0 = sum_t lambda_{k+1}[tau0_t] v_t,       dZ/dm1 = sum_t s_t lambda_{k+1}[tau1_t] v_t,
+// with lambda_ns = 1 at the final entry.  Each coset reads and writes only its own slots, so the reverse pass is
+// in place and race-free like the forward one.  The reverse pass needs T_k: the forward sweep keeps a compact copy
+// of the live table ([coset][offset], 2^{r_k} entries) every `every` steps, and each segment between two
+// checkpoints is recomputed forward once, keeping its tables, before the reverse pass walks it.  Per string the
+// whole sequence (forward, then per segment: restore, recompute, reverse) is one CUDA graph; the string index lives
+// in device memory and advances at its end.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gsb.h"
+#include "gsb_common.h"
+#include "gsb_plan.h"
+#include "gsb_step.h"
+
+namespace gsb {
+
+struct GradCtx {
+    const double *M;         // [ns][2][2] (re, im): the caller's matrices
+    const int8_t *bits;      // [cap][ns]
+    const int *item;         // current string
+    int ns;
+};
+
+__device__ __forceinline__ uint64_t coset_base(const StepArgs &s, uint64_t c) {
+    uint64_t b = 0;
+    while (c) {
+        const int j = __ffsll((long long)c) - 1;
+        b ^= s.tk[j];
+        c &= c - 1;
+    }
+    return b;
+}
+
+__device__ __forceinline__ void step_row(const StepArgs &s, const GradCtx &g, double2 &m0, double2 &m1) {
+    const int b = g.bits[(size_t)*g.item * (size_t)g.ns + (size_t)s.k];
+    const double *Mk = g.M + (size_t)s.k * 8 + 4 * b;
+    m0 = make_double2(Mk[0], Mk[1]);
+    m1 = make_double2(Mk[2], Mk[3]);
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+    return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
+
+__global__ void k_gr_begin(double2 *T) { T[0] = make_double2(1.0, 0.0); }
+
+// Forward step on the T arena: gathers the input table to `gather` ([c][t], if given) and, if `write`, stores the
+// step's outputs in place.
+__global__ void __launch_bounds__(256) k_gr_fwd(const StepArgs s, double2 *__restrict__ T, double2 *__restrict__ gather,
+                                                int write, const GradCtx g) {
+    double2 m0, m1;
+    step_row(s, g, m0, m1);
+    const uint64_t N = 1ULL << s.nk;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = coset_base(s, c);
+        const int pc = __popcll(c & s.rhoc) & 1;
+        double2 v[4];
+        for (int t = 0; t < s.ntq; t++) v[t] = T[base ^ s.tq[t]];
+        if (gather)
+            for (int t = 0; t < s.ntq; t++) gather[c * (uint64_t)s.ntq + (uint64_t)t] = v[t];
+        if (!write) continue;
+        double2 o[2] = {make_double2(0, 0), make_double2(0, 0)};
+        for (int t = 0; t < s.ntq; t++) {
+            o[s.tau0[t]] = cadd(o[s.tau0[t]], cmul(m0, v[t]));
+            o[s.tau1[t]] = cadd(o[s.tau1[t]], cscale((pc ^ s.par[t]) ? -1.0 : 1.0, cmul(m1, v[t])));
+        }
+        T[base] = o[0];
+        if (s.m == 2) T[base ^ s.g] = o[1];
+    }
+}
+
+// Restore a checkpoint: the compact table [c][t] back to its arena slots.
+__global__ void __launch_bounds__(256) k_gr_scatter(const StepArgs s, const double2 *__restrict__ src, double2 *__restrict__ T) {
+    const uint64_t N = 1ULL << s.nk;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = coset_base(s, c);
+        for (int t = 0; t < s.ntq; t++) T[base ^ s.tq[t]] = src[c * (uint64_t)s.ntq + (uint64_t)t];
+    }
+}
+
+// End of the forward sweep: Z = T[0]; lambda_ns = 1.
+__global__ void k_gr_final(const double2 *T, double2 *Lam, double2 *z_out, const int *item) {
+    z_out[*item] = T[0];
+    Lam[0] = make_double2(1.0, 0.0);
+}
+
+__global__ void k_gr_next(int *item) { *item += 1; }
+__global__ void k_gr_set_item(int *item, int v) { *item = v; }
+
+// Reverse step: lambda_{k+1} (output slots of the Lam arena) -> lambda_k (input slots, in place), and
+// dZ/dM_k[b_k][x] from the step's input table Tk ([c][t]).  Deterministic reduction: per-block partials, the last
+// block sums them in block order and writes grad[item][k] = (dZ/dm0, dZ/dm1).
+__global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 *__restrict__ Tk, double2 *__restrict__ Lam,
+                                                const GradCtx g, double *partials, unsigned int *counter, double *grad) {
+    double2 m0, m1;
+    step_row(s, g, m0, m1);
+    const uint64_t N = 1ULL << s.nk;
+    double a[4] = {0, 0, 0, 0};   // dZ/dm0 (re, im), dZ/dm1 (re, im)
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t base = coset_base(s, c);
+        const int pc = __popcll(c & s.rhoc) & 1;
+        const double2 lam[2] = {Lam[base], s.m == 2 ? Lam[base ^ s.g] : make_double2(0, 0)};
+        double2 nl[4];
+        for (int t = 0; t < s.ntq; t++) {
+            const double2 v = Tk[c * (uint64_t)s.ntq + (uint64_t)t];
+            const double sg = (pc ^ s.par[t]) ? -1.0 : 1.0;
+            const double2 la = lam[s.tau0[t]], lb = cscale(sg, lam[s.tau1[t]]);
+            const double2 p0 = cmul(la, v), p1 = cmul(lb, v);
+            a[0] += p0.x;
+            a[1] += p0.y;
+            a[2] += p1.x;
+            a[3] += p1.y;
+            nl[t] = cadd(cmul(m0, la), cmul(m1, lb));
+        }
+        for (int t = 0; t < s.ntq; t++) Lam[base ^ s.tq[t]] = nl[t];
+    }
+    __shared__ double red[4][8];
+    __shared__ int last;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    for (int i = 0; i < 4; i++) a[i] = warp_sum(a[i]);
+    if (lane == 0)
+        for (int i = 0; i < 4; i++) red[i][warp] = a[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 4; i++) {
+            double t = 0;
+            for (int w = 0; w < nw; w++) t += red[i][w];
+            partials[4 * blockIdx.x + i] = t;
+        }
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double t[4] = {0, 0, 0, 0};
+    for (unsigned int b = 0; b < gridDim.x; b++)
+        for (int i = 0; i < 4; i++) t[i] += __ldcg(partials + 4 * b + i);
+    double *out = grad + ((size_t)*g.item * (size_t)g.ns + (size_t)s.k) * 4;
+    for (int i = 0; i < 4; i++) out[i] = t[i];
+    *counter = 0;
+}
+
+struct GradEngine {
+    HPlan plan;
+    int dev = 0, sms = 0, every = 4, cap = 1024;
+    std::vector<StepArgs> args;
+    std::vector<size_t> ckpt_off;      // offset (entries) of step k's checkpoint in d_ckpt (k % every == 0)
+    double2 *T = nullptr, *Lam = nullptr, *d_ckpt = nullptr, *d_seg = nullptr;
+    size_t seg_stride = 0;             // entries per segment table
+    double *d_M = nullptr, *partials = nullptr, *d_grad = nullptr;
+    double2 *d_z = nullptr;
+    int8_t *d_bits = nullptr;
+    int *d_item = nullptr;
+    unsigned int *d_counter = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int maxgrid = 1;
+
+    ~GradEngine() {
+        int prev = 0;
+        cudaGetDevice(&prev);
+        cudaSetDevice(dev);
+        if (graph) cudaGraphExecDestroy(graph);
+        cudaFree(T);
+        cudaFree(Lam);
+        cudaFree(d_ckpt);
+        cudaFree(d_seg);
+        cudaFree(d_M);
+        cudaFree(partials);
+        cudaFree(d_grad);
+        cudaFree(d_z);
+        cudaFree(d_bits);
+        cudaFree(d_item);
+        cudaFree(d_counter);
+        if (stream) cudaStreamDestroy(stream);
+        cudaSetDevice(prev);
+    }
+
+    int grid_of(const StepArgs &s) const {
+        const uint64_t N = 1ULL << s.nk;
+        return (int)std::max<uint64_t>(1, std::min<uint64_t>((N + 255) / 256, (uint64_t)maxgrid));
+    }
+    GradCtx ctx() const { return GradCtx{d_M, d_bits, d_item, plan.ns}; }
+    double2 *seg(int pos) const { return d_seg + (size_t)(pos - 1) * seg_stride; }   // pos = 1 .. every-1
+
+    // The per-string sequence (captured once as a graph).
+    cudaError_t enqueue() {
+        const int ns = plan.ns;
+        const GradCtx g = ctx();
+        k_gr_begin<<<1, 1, 0, stream>>>(T);
+        for (int k = 0; k < ns; k++) {
+            const StepArgs &s = args[(size_t)k];
+            k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, k % every == 0 ? d_ckpt + ckpt_off[(size_t)k] : nullptr, 1, g);
+        }
+        k_gr_final<<<1, 1, 0, stream>>>(T, Lam, d_z, d_item);
+        for (int c = ((ns - 1) / every) * every; c >= 0; c -= every) {
+            const int e = std::min(c + every, ns);
+            const StepArgs &sc = args[(size_t)c];
+            k_gr_scatter<<<grid_of(sc), 256, 0, stream>>>(sc, d_ckpt + ckpt_off[(size_t)c], T);
+            for (int j = c; j < e; j++) {   // recompute: gather T_j (j > c), write T_{j+1} (j < e - 1)
+                if (j == c && e - 1 == c) break;
+                const StepArgs &s = args[(size_t)j];
+                k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, j == c ? nullptr : seg(j - c), j < e - 1 ? 1 : 0, g);
+            }
+            for (int j = e - 1; j >= c; j--) {
+                const StepArgs &s = args[(size_t)j];
+                const double2 *tk = j == c ? d_ckpt + ckpt_off[(size_t)c] : seg(j - c);
+                k_gr_bwd<<<grid_of(s), 256, 0, stream>>>(s, tk, Lam, g, partials, d_counter, d_grad);
+            }
+        }
+        k_gr_next<<<1, 1, 0, stream>>>(d_item);
+        return cudaGetLastError();
+    }
+};
+
+}  // namespace gsb
+
+using namespace gsb;
+
+#define GR_CK(x)                                                                                                  \
+    do {                                                                                                          \
+        cudaError_t e_ = (x);                                                                                     \
+        if (e_ != cudaSuccess) return fail(GSB_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #x); \
+    } while (0)
+
+struct gsb_grad {
+    GradEngine E;
+};
+
+extern "C" {
+
+int gsb_grad_open_text(const char *text, size_t len, int device, int every, gsb_grad **out) {
+    if (!text || !out) return fail(GSB_E_USAGE, "null argument");
+    *out = nullptr;
+    if (every < 1 || every > 64) return fail(GSB_E_USAGE, "checkpoint interval must be 1..64");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return fail(GSB_E_CUDA, "no CUDA device is visible");
+    if (device < 0 || device >= ndev) return fail(GSB_E_USAGE, "device out of range");
+    gsb_grad *h = new gsb_grad();
+    GradEngine &E = h->E;
+    std::string err;
+    int rc = parse_plan_text(text, len, E.plan, err);
+    if (!rc) rc = validate_plan(E.plan, err);
+    if (rc) {
+        delete h;
+        return fail(rc, err);
+    }
+    const HPlan &p = E.plan;
+    if (p.ns < 1) {
+        delete h;
+        return fail(GSB_E_USAGE, "plan has no steps");
+    }
+    const HStep &lastst = p.st[(size_t)p.ns - 1];
+    if (lastst.nk != 0 || lastst.m != 1) {
+        delete h;
+        return fail(GSB_E_USAGE, "the last step must leave a single entry (nk = 0, m = 1)");
+    }
+    E.dev = device;
+    E.every = every;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    struct Restore {
+        int p;
+        ~Restore() { cudaSetDevice(p); }
+    } restore{prev};
+    cudaDeviceGetAttribute(&E.sms, cudaDevAttrMultiProcessorCount, device);
+    E.maxgrid = std::max(1, E.sms * 8);
+    E.args.resize((size_t)p.ns);
+    E.ckpt_off.assign((size_t)p.ns, 0);
+    size_t ck = 0, maxr = 0;
+    for (int k = 0; k < p.ns; k++) {
+        const HStep &s = p.st[(size_t)k];
+        StepArgs a;
+        memset(&a, 0, sizeof a);
+        for (int j = 0; j < s.nk; j++) a.tk[j] = s.tk[(size_t)j];
+        a.ntq = (int)s.tqs.size();
+        for (int i = 0; i < a.ntq; i++) {
+            a.tq[i] = s.tqs[(size_t)i];
+            a.tau0[i] = s.tau0[i];
+            a.tau1[i] = s.tau1[i];
+            a.par[i] = s.par[i];
+        }
+        a.g = s.m == 2 ? s.g : 0;
+        a.rhoc = s.rhoc;
+        a.nk = s.nk;
+        a.k = k;
+        a.m = s.m;
+        E.args[(size_t)k] = a;
+        const size_t entries = ((size_t)1 << s.nk) * (size_t)a.ntq;
+        maxr = std::max(maxr, entries);
+        if (k % every == 0) {
+            E.ckpt_off[(size_t)k] = ck;
+            ck += entries;
+        }
+    }
+    E.seg_stride = maxr;
+    const size_t arena = (size_t)1 << p.R;
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t need = 16 * (2 * arena + ck + (size_t)std::max(0, every - 1) * maxr);
+    if (need > free_b / 10 * 9) {
+        delete h;
+        return fail(GSB_E_ALLOC, "arena, checkpoints and segment tables need " + std::to_string(need) +
+                                     " bytes; the device has " + std::to_string(free_b) + " free");
+    }
+    cudaError_t e = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&E.T, arena * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.Lam, arena * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_ckpt, std::max<size_t>(ck, 1) * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_seg, std::max<size_t>((size_t)std::max(0, every - 1) * maxr, 1) * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_M, (size_t)p.ns * 8 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&E.partials, (size_t)E.maxgrid * 4 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_grad, (size_t)E.cap * (size_t)p.ns * 4 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_z, (size_t)E.cap * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_bits, (size_t)E.cap * (size_t)p.ns);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_item, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_counter, sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(E.d_counter, 0, sizeof(unsigned int), E.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(E.T, 0, arena * 16, E.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(E.Lam, 0, arena * 16, E.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
+    if (e != cudaSuccess) {
+        delete h;
+        return fail(GSB_E_ALLOC, std::string("device allocation: ") + cudaGetErrorString(e));
+    }
+    *out = h;
+    return 0;
+}
+
+int gsb_grad_close(gsb_grad *h) {
+    delete h;
+    return 0;
+}
+
+int gsb_grad_run(gsb_grad *h, const double *M, const int8_t *bits, int64_t nstr, double *z, double *dz) {
+    if (!h) return fail(GSB_E_STATE, "null handle");
+    if (nstr < 0 || (nstr && (!M || !bits || !z || !dz))) return fail(GSB_E_USAGE, "null argument");
+    GradEngine &E = h->E;
+    const int ns = E.plan.ns;
+    for (int64_t i = 0; i < nstr * ns; i++)
+        if (bits[i] != 0 && bits[i] != 1) return fail(GSB_E_USAGE, "bits must be 0 or 1");
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(E.dev);
+    struct Restore {
+        int p;
+        ~Restore() { cudaSetDevice(p); }
+    } restore{prev};
+    GR_CK(cudaMemcpyAsync(E.d_M, M, (size_t)ns * 8 * sizeof(double), cudaMemcpyHostToDevice, E.stream));
+    if (!E.graph) {
+        cudaGraph_t gr = nullptr;
+        GR_CK(cudaStreamBeginCapture(E.stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = E.enqueue();
+        cudaError_t e2 = cudaStreamEndCapture(E.stream, &gr);
+        if (e != cudaSuccess) {
+            if (gr) cudaGraphDestroy(gr);
+            GR_CK(e);
+        }
+        GR_CK(e2);
+        e = cudaGraphInstantiate(&E.graph, gr, 0);
+        cudaGraphDestroy(gr);
+        GR_CK(e);
+    }
+    for (int64_t off = 0; off < nstr; off += E.cap) {
+        const int64_t nb = std::min<int64_t>(E.cap, nstr - off);
+        GR_CK(cudaMemcpyAsync(E.d_bits, bits + off * ns, (size_t)(nb * ns), cudaMemcpyHostToDevice, E.stream));
+        k_gr_set_item<<<1, 1, 0, E.stream>>>(E.d_item, 0);
+        GR_CK(cudaGetLastError());
+        for (int64_t i = 0; i < nb; i++) GR_CK(cudaGraphLaunch(E.graph, E.stream));
+        GR_CK(cudaMemcpyAsync(z + 2 * off, E.d_z, (size_t)nb * 16, cudaMemcpyDeviceToHost, E.stream));
+        GR_CK(cudaMemcpyAsync(dz + off * ns * 4, E.d_grad, (size_t)(nb * ns) * 4 * sizeof(double),
+                              cudaMemcpyDeviceToHost, E.stream));
+        GR_CK(cudaStreamSynchronize(E.stream));
+    }
+    return 0;
+}
+
+int gsb_grad_info(const gsb_grad *h, int *n, int *nsteps, int *R) {
+    if (!h) return fail(GSB_E_STATE, "null handle");
+    if (n) *n = h->E.plan.n;
+    if (nsteps) *nsteps = h->E.plan.ns;
+    if (R) *R = h->E.plan.R;
+    return 0;
+}
+
+}  // extern "C"

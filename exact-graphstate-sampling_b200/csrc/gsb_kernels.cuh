@@ -24,21 +24,14 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "gsb_step.h"
+
 namespace gsb {
 
 enum Driver : int {
     DRV_CHAIN = 0,   // normalised: norm pass, draw/force, write with 1/sqrt(n_b)      (gsamp2.cpp:39-55)
     DRV_CHAIN1 = 1,  // one pass, unnormalised storage, cond = nb / (2 prev)         (gsamp2.cpp:59-70)
     DRV_HYBRID = 2,  // lazily rescaled run_steps: optional norm pass, write with 1/sqrt(prev)   (gsamp2.cpp:77-98)
-};
-
-struct StepArgs {
-    uint64_t tk[40];        // Tkeep (entries >= nk are 0)
-    uint64_t tq[4];         // distinct coset offsets, ascending
-    uint64_t g, rhoc;
-    double Mr[2][2], Mi[2][2];
-    int nk, k, ntq, m;
-    int tau0[4], tau1[4], par[4];
 };
 
 struct DevState {
@@ -96,11 +89,6 @@ __device__ __forceinline__ uint64_t xor_cols(const uint64_t *tks, uint64_t c) {
     return a;
 }
 
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 // Block-wide sum of (a0, a1) into partials[blockIdx]; returns true in thread 0 of the last block to finish, with
 // the grid totals in (t0, t1).  All threads of the block must call it.

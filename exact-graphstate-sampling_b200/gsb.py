@@ -70,6 +70,10 @@ def _load():
         "gsb_dp_extend": (c.c_int, [c.c_int, c.c_int, c.c_uint64, c.c_uint64, c.c_int, u64p, dp, dp, dp, c.c_int]),
         "gsb_dp_extend_static": (c.c_int, [c.c_int, c.c_int, c.c_uint64, c.c_uint64, c.c_int, u64p, dp, dp, dp,
                                            c.c_int]),
+        "gsb_grad_open_text": (c.c_int, [c.c_char_p, c.c_size_t, c.c_int, c.c_int, c.POINTER(P)]),
+        "gsb_grad_close": (c.c_int, [P]),
+        "gsb_grad_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+        "gsb_grad_run": (c.c_int, [P, dp, c.POINTER(c.c_int8), c.c_int64, dp, dp]),
         "gsb_validate_text": (c.c_int, [c.c_char_p, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
                                         c.POINTER(c.c_int)]),
         "gsb_cut_profile": (c.c_int, [c.c_int, c.POINTER(c.c_uint8), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
@@ -89,7 +93,8 @@ EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "g
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
            "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
-           "gsb_dp_extend", "gsb_dp_extend_static")
+           "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
+           "gsb_grad_run")
 
 
 def lib():
@@ -283,6 +288,11 @@ class Engine:
         M = np.array([[float(x) for x in r[-8:]] for r in rows], np.float64).reshape(-1)
         _check(_lib.gsb_set_matrices(self.handle, _ptr(np.ascontiguousarray(M), ctypes.c_double)))
 
+    def set_matrices(self, M):
+        """Replace every step's matrix: M [ns][2][2] complex, step order (same plan layout)."""
+        Mc = np.ascontiguousarray(M, np.complex128).reshape(self.ns, 2, 2)
+        _check(_lib.gsb_set_matrices(self.handle, _ptr(Mc.view(np.float64), ctypes.c_double)))
+
     def set_fusion(self, depth):
         """'chain' mode: fuse up to `depth` consecutive wide steps per pass (1 = no fusion)."""
         _check(_lib.gsb_set_fusion(self.handle, int(depth)))
@@ -354,6 +364,43 @@ class DpEngine:
 
     def __exit__(self, *exc):
         self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GradSweep:
+    """The adjoint sweep (complex128) on one in-place plan: Z(b) and dZ/dM_k[b_k][x] for a batch of strings."""
+
+    def __init__(self, plan_text, device=0, every=4):
+        h = ctypes.c_void_p()
+        b = plan_text.encode() if isinstance(plan_text, str) else bytes(plan_text)
+        _check(_lib.gsb_grad_open_text(b, len(b), int(device), int(every), ctypes.byref(h)))
+        self._h = h
+        n, ns, R = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(_lib.gsb_grad_info(h, ctypes.byref(n), ctypes.byref(ns), ctypes.byref(R)))
+        self.n, self.ns, self.R = n.value, ns.value, R.value
+
+    def run(self, M, bits):
+        """M: [ns][2][2] complex (step order); bits: [nstr][ns] (step order).  Returns (Z [nstr] complex128,
+        dZ [nstr][ns][2] complex128 with dZ[s, k, x] = dZ(b_s)/dM_k[b_sk][x])."""
+        Mc = np.ascontiguousarray(M, np.complex128).reshape(self.ns, 2, 2)
+        b = as_bits(bits, self.ns)
+        z = np.zeros(max(len(b), 1), np.complex128)
+        dz = np.zeros((max(len(b), 1), self.ns, 2), np.complex128)
+        if len(b):
+            _check(_lib.gsb_grad_run(self._h, _ptr(Mc.view(np.float64), ctypes.c_double), _ptr(b, ctypes.c_int8),
+                                     len(b), _ptr(z.view(np.float64), ctypes.c_double),
+                                     _ptr(dz.view(np.float64), ctypes.c_double)))
+        return z[:len(b)], dz[:len(b)]
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.gsb_grad_close(self._h)
+            self._h = None
 
     def __del__(self):
         try:

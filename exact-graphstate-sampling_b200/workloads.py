@@ -29,6 +29,25 @@ def matching_instance(n=70, depth=70, seed=2, order_seed=12, iters=60000):
                 steps=st)
 
 
+def rotation_instance(n, depth=None, seed=0, order_seed=12, iters=60000):
+    """The matching construction with its U3 layer as parameters (the differentiation workload).
+
+    The plan is built from the Clifford body alone, so its matrices are M0_j = U_j^dag (the graph form's local
+    Cliffords), and the layer's Haar angles theta0 [n, 3] are returned beside it: the step matrices of the full
+    circuit are U3(theta_v) M0_v (adjoint.step_matrices)."""
+    n, body, tail = circuits.matching_circuit(n, depth, seed=seed)
+    from graphform import graph_form
+    A, _ = graph_form(circuits.tableau_of(n, body))
+    order, w = gsb.order_search(A, seed=order_seed, ngreedy=4, iters=iters)
+    am = Amplitudes(n, circuits.tableau_of(n, body), [], order)
+    R = max(1, plan_width(am.steps))
+    st = plan_inplace(am.A, order, R)
+    theta0 = np.array([[float(x) for x in name[3:-1].split(",")] for name, _ in tail])
+    return dict(name=f"rotations_n{n}_d{n if depth is None else depth}_s{seed}", n=n, body=body, tail=tail,
+                order=order, width=R, plan=inplace_plan_text(st, R, am.M, n), steps=st, M0=np.array(am.M),
+                theta0=theta0, step_vertices=[int(x["v"]) for x in st])
+
+
 def matching_n70_w30():
     return matching_instance(70, 70, 2, 12, 60000)
 

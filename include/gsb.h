@@ -162,6 +162,18 @@ int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const
 int gsb_dp_extend_static(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const uint64_t *ker,
                          const double *wv, const double *old_table, double *new_table, int device);
 
+/* ---- adjoint sweep: gradients of log Pr(b) with respect to the step matrices (complex128) ----
+ * No counterpart in the reference (it has no differentiation).  The plan text is the in-place plan (its own M
+ * values are ignored: every run takes the matrices).  `every` is the checkpoint interval in steps; the segment
+ * between two checkpoints is recomputed once during the reverse sweep. */
+typedef struct gsb_grad gsb_grad;
+int gsb_grad_open_text(const char *plan_text, size_t len, int device, int every, gsb_grad **out);
+int gsb_grad_close(gsb_grad *g);
+int gsb_grad_info(const gsb_grad *g, int *n, int *nsteps, int *R);
+/* M [nsteps][2][2] complex (re, im), step order; bits [nstr][nsteps] in step order.  Outputs: z [nstr] complex, the
+ * sweep's final value Z(b) (Pr(b) = 2^-n |Z(b)|^2), and dz [nstr][nsteps][2] complex, dZ/dM_k[b_k][x]. */
+int gsb_grad_run(gsb_grad *g, const double *M, const int8_t *bits, int64_t nstr, double *z, double *dz);
+
 /* ---- host-side helpers (no GPU needed) ---- */
 
 /* Parse and validate a plan without allocating anything on a device: the same checks gsb_open_* makes
