@@ -74,6 +74,15 @@ def _load():
         "gsb_grad_close": (c.c_int, [P]),
         "gsb_grad_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_grad_run": (c.c_int, [P, dp, c.POINTER(c.c_int8), c.c_int64, dp, dp]),
+        "gsb_batch_open": (c.c_int, [c.POINTER(c.c_char_p), c.POINTER(c.c_size_t), c.c_int, c.c_int, c.c_int,
+                                     c.POINTER(P)]),
+        "gsb_batch_close": (c.c_int, [P]),
+        "gsb_batch_set_strings": (c.c_int, [P, c.POINTER(c.c_int), c.c_int, c.c_int, i8p, i8p]),
+        "gsb_batch_run": (c.c_int, [P, dp, c.POINTER(c.c_float)]),
+        "gsb_batch_set_shape": (c.c_int, [P, c.c_int, c.c_int, c.c_int]),
+        "gsb_batch_get_shape": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
+        "gsb_batch_tune": (c.c_int, [P, c.c_int, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
+                                     c.POINTER(c.c_int), c.POINTER(c.c_float)]),
         "gsb_validate_text": (c.c_int, [c.c_char_p, c.c_size_t, c.POINTER(c.c_int), c.POINTER(c.c_int),
                                         c.POINTER(c.c_int)]),
         "gsb_cut_profile": (c.c_int, [c.c_int, c.POINTER(c.c_uint8), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
@@ -94,7 +103,8 @@ EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "g
            "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
-           "gsb_grad_run")
+           "gsb_grad_run", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
+           "gsb_batch_set_shape", "gsb_batch_get_shape", "gsb_batch_tune")
 
 
 def lib():
@@ -400,6 +410,64 @@ class GradSweep:
     def close(self):
         if getattr(self, "_h", None) is not None:
             _lib.gsb_grad_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Batch:
+    """Many instances (in-place plans of uneven width) in one persistent launch; strings share prefixes."""
+
+    def __init__(self, plan_texts, precision=GSB_C64, device=0):
+        bs = [t.encode() if isinstance(t, str) else bytes(t) for t in plan_texts]
+        arr = (ctypes.c_char_p * len(bs))(*bs)
+        lens = (ctypes.c_size_t * len(bs))(*[len(b) for b in bs])
+        h = ctypes.c_void_p()
+        _check(_lib.gsb_batch_open(arr, lens, len(bs), int(precision), int(device), ctypes.byref(h)))
+        self._h = h
+        self.ninst = len(bs)
+        self._shape = None
+
+    def set_strings(self, K, prefixes, suffixes):
+        """K[i]: prefix length; prefixes[i]: [npre][K[i]]; suffixes[i]: [npre][nsuf][ns_i - K[i]] (0/1, step order)."""
+        pre = [np.ascontiguousarray(p, np.int8) for p in prefixes]
+        suf = [np.ascontiguousarray(s, np.int8) for s in suffixes]
+        self.npre, self.nsuf = pre[0].shape[0], suf[0].shape[1]
+        Kc = np.ascontiguousarray(K, np.int32)
+        pb = np.concatenate([p.reshape(-1) for p in pre])
+        sb = np.concatenate([s.reshape(-1) for s in suf])
+        _check(_lib.gsb_batch_set_strings(self._h, _ptr(Kc, ctypes.c_int), self.npre, self.nsuf,
+                                          _ptr(pb, ctypes.c_int8), _ptr(sb, ctypes.c_int8)))
+
+    def run(self):
+        """(log2 Pr [ninst][npre][nsuf], device milliseconds of the launch)."""
+        out = np.zeros(self.ninst * self.npre * self.nsuf)
+        ms = ctypes.c_float()
+        _check(_lib.gsb_batch_run(self._h, _ptr(out, ctypes.c_double), ctypes.byref(ms)))
+        return out.reshape(self.ninst, self.npre, self.nsuf), ms.value
+
+    def set_shape(self, block, small_R, per_sm):
+        _check(_lib.gsb_batch_set_shape(self._h, int(block), int(small_R), int(per_sm)))
+
+    def shape(self):
+        v = [ctypes.c_int() for _ in range(3)]
+        _check(_lib.gsb_batch_get_shape(self._h, *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    def tune(self, reps=2, max_bytes=8 << 30):
+        """Autotune the launch shape on the current strings; returns (block, small_R, per_sm, mean ms)."""
+        v = [ctypes.c_int() for _ in range(3)]
+        ms = ctypes.c_float()
+        _check(_lib.gsb_batch_tune(self._h, int(reps), int(max_bytes), *[ctypes.byref(x) for x in v], ctypes.byref(ms)))
+        return tuple(x.value for x in v) + (ms.value,)
+
+    def close(self):
+        if getattr(self, "_h", None) is not None:
+            _lib.gsb_batch_close(self._h)
             self._h = None
 
     def __del__(self):

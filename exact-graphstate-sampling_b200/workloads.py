@@ -48,6 +48,24 @@ def rotation_instance(n, depth=None, seed=0, order_seed=12, iters=60000):
                 theta0=theta0, step_vertices=[int(x["v"]) for x in st])
 
 
+def batch_workload(count=512, seed=0, nmin=16, nmax=40, npre=16, nsuf=4, iters=5000):
+    """The batched workload: `count` matching instances with n uniform in [nmin, nmax] (instance i: circuit seed
+    seed * 100003 + i, order seed 12), and per instance npre random prefixes over its first floor(ns/2) steps, each
+    with nsuf random suffixes.  Returns dict(instances, K, prefixes, suffixes)."""
+    rng = np.random.default_rng(seed)
+    ns_list = rng.integers(nmin, nmax + 1, size=count)
+    inst, K, pre, suf = [], [], [], []
+    for i, n in enumerate(ns_list):
+        w = matching_instance(int(n), int(n), seed * 100003 + i, 12, iters)
+        ns = len(w["steps"])
+        k = ns // 2
+        inst.append(w)
+        K.append(k)
+        pre.append(rng.integers(0, 2, size=(npre, k), dtype=np.int8))
+        suf.append(rng.integers(0, 2, size=(npre, nsuf, ns - k), dtype=np.int8))
+    return dict(instances=inst, K=K, prefixes=pre, suffixes=suf)
+
+
 def matching_n70_w30():
     return matching_instance(70, 70, 2, 12, 60000)
 

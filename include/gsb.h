@@ -174,6 +174,27 @@ int gsb_grad_info(const gsb_grad *g, int *n, int *nsteps, int *R);
  * sweep's final value Z(b) (Pr(b) = 2^-n |Z(b)|^2), and dz [nstr][nsteps][2] complex, dZ/dM_k[b_k][x]. */
 int gsb_grad_run(gsb_grad *g, const double *M, const int8_t *bits, int64_t nstr, double *z, double *dz);
 
+/* ---- batched instances: one persistent launch over many plans of uneven width ----
+ * No counterpart in the reference (its executor runs one plan per process).  Each instance is an in-place plan
+ * (width <= 24); strings are npre prefixes of K[i] bits per instance, each followed by nsuf suffixes of
+ * ns_i - K[i] bits (step order): the prefix is evaluated once and every suffix resumes from its table.
+ * precision: GSB_C64 (complex64 arena, FP32 sums, FP64 norms and scales) or GSB_C128. */
+typedef struct gsb_batch gsb_batch;
+int gsb_batch_open(const char *const *plan_texts, const size_t *lens, int ninst, int precision, int device,
+                   gsb_batch **out);
+int gsb_batch_close(gsb_batch *b);
+/* prefix_bits: concatenation over instances of [npre][K[i]]; suffix_bits: of [npre][nsuf][ns_i - K[i]]. */
+int gsb_batch_set_strings(gsb_batch *b, const int *K, int npre, int nsuf, const int8_t *prefix_bits,
+                          const int8_t *suffix_bits);
+/* log2p: concatenation over instances of [npre][nsuf]; ms (may be NULL): device time of the launch. */
+int gsb_batch_run(gsb_batch *b, double *log2p, float *ms);
+/* Launch shape: threads per CTA, widest instance run by a single warp (narrower ones too), CTAs per SM. */
+int gsb_batch_set_shape(gsb_batch *b, int block, int small_R, int per_sm);
+int gsb_batch_get_shape(const gsb_batch *b, int *block, int *small_R, int *per_sm);
+/* Autotuner: times the candidate shapes on the current strings (reps timed runs each, arenas <= max_bytes) and
+ * keeps the fastest; returns it and its mean time. */
+int gsb_batch_tune(gsb_batch *b, int reps, size_t max_bytes, int *block, int *small_R, int *per_sm, float *best_ms);
+
 /* ---- host-side helpers (no GPU needed) ---- */
 
 /* Parse and validate a plan without allocating anything on a device: the same checks gsb_open_* makes

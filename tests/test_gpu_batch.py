@@ -1,0 +1,64 @@
+"""Batched persistent launch (gsb_batch_*): many instances of uneven width, strings sharing prefixes.
+
+Every (prefix, suffix) string's log2 Pr equals the single-plan executor's 'chain' on the concatenated string
+(complex128: <= 1e-9), the complex64 form stays within the stated tolerance of complex128, and the result does not
+depend on the launch shape (block size, warp/CTA split, CTAs per SM) or on the autotuner's choice.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    import workloads
+    return workloads.batch_workload(count=14, seed=3, nmin=16, nmax=30, npre=3, nsuf=2, iters=2000)
+
+
+def _strings(bw, i):
+    p, s = bw["prefixes"][i], bw["suffixes"][i]
+    return np.array([np.concatenate([p[a], s[a, b]]) for a in range(p.shape[0]) for b in range(s.shape[1])], np.int8)
+
+
+def test_batch_c128_equals_executor(small_batch):
+    import gsb
+    bw = small_batch
+    b = gsb.Batch([w["plan"] for w in bw["instances"]], precision=gsb.GSB_C128)
+    b.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+    lp, ms = b.run()
+    worst = 0.0
+    for i, w in enumerate(bw["instances"]):
+        with gsb.Engine.from_text(w["plan"], precision=gsb.GSB_C128) as eng:
+            want = eng.chain(_strings(bw, i))[0]
+        got = lp[i].reshape(-1)
+        fin = np.isfinite(want)
+        assert (np.isfinite(got) == fin).all()
+        worst = max(worst, float(np.max(np.abs(got[fin] - want[fin]), initial=0.0)))
+    assert worst <= 1e-9, worst
+    assert ms > 0
+
+
+def test_batch_shapes_and_c64(small_batch):
+    import gsb
+    bw = small_batch
+    plans = [w["plan"] for w in bw["instances"]]
+    ref = gsb.Batch(plans, precision=gsb.GSB_C128)
+    ref.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+    want, _ = ref.run()
+    b = gsb.Batch(plans, precision=gsb.GSB_C64)
+    b.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+    outs = []
+    for shape in [(256, 12, 2), (128, 0, 1), (512, 16, 1), (256, 8, 4)]:
+        b.set_shape(*shape)
+        outs.append(b.run()[0])
+        assert b.shape() == shape
+    for o in outs[1:]:
+        assert np.max(np.abs(o - outs[0])) <= 1e-5     # complex64 sums in a shape-dependent order
+    tuned = b.tune(reps=1)
+    assert len(tuned) == 4 and tuned[3] > 0
+    got, _ = b.run()
+    d = np.abs(got - want)
+    # complex64 (FP32 sums, FP64 norms and scales) against complex128; log2 amplifies the rounding of unlikely
+    # strings, so the bound scales with -log2 Pr
+    assert np.all(d <= 2e-5 * np.maximum(1.0, -want / 10)), float(d.max())
