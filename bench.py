@@ -21,6 +21,13 @@ own strings on its own GPU; value = all ranks' amplitudes / the slowest rank's t
 
 --impl reference times the reference's own CPU executor (gsamp2 compiled from its sources into oracle/_ref, complex64,
 'chain' mode, every host core) on one string of the same workload per step, on rank 0 only.
+
+--form batch|grad|wide34 measures the other workloads instead, one JSON line each (1 GPU):
+  batch : 512 matching instances, n uniform in [16, 40], 16 prefixes x 4 suffixes each, one persistent launch
+          (complex64, autotuned shape, complex128 agreement);
+  grad  : n = 48 rotation layer, loss -mean log2 Pr over 2048 targets drawn exactly from a second instance,
+          gradient by the adjoint sweep;
+  wide34: n = 80, width 34 (2^34-entry complex64 arena, 137 GB): 256 amplitudes and 16 exact samples.
 """
 import argparse
 import json
@@ -62,6 +69,9 @@ def parse():
     ap.add_argument("--profile-mode", default="chain", choices=["chain", "sample"],
                     help="with --profile-chain: evaluate strings (chain) or draw exact samples (sample)")
     ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 128])
+    ap.add_argument("--form", default="headline", choices=["headline", "batch", "grad", "wide34"],
+                    help="workload to measure (the default line is the headline n = 70, width-30 workload)")
+    ap.add_argument("--batch-instances", type=int, default=512)
     return ap.parse_args()
 
 
@@ -365,9 +375,136 @@ def run_gsb(args):
     replicas.finish(world)
 
 
+def _form_line(form, metric, value, unit, hib, extra):
+    d = {"form": form, "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "higher_is_better": hib,
+         "data": "synthetic"}
+    d.update(extra)
+    print(json.dumps(d), flush=True)
+
+
+def run_form_batch(args):
+    """Batched uneven workload: one persistent launch over all (instance, prefix) items."""
+    import numpy as np
+    import gsb
+    import workloads
+    t0 = time.perf_counter()
+    bw = workloads.batch_workload(count=args.batch_instances, seed=0, npre=16, nsuf=4)
+    t_plan = time.perf_counter() - t0
+    plans = [w["plan"] for w in bw["instances"]]
+    widths = [w["width"] for w in bw["instances"]]
+    b = gsb.Batch(plans, precision=gsb.GSB_C64)
+    b.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+    block, small_R, per_sm, tune_ms = b.tune(reps=2)
+    for _ in range(max(3, args.warmup)):
+        b.run()
+    times = []
+    for _ in range(args.steps):
+        lp, ms = b.run()
+        times.append(ms)
+    ms = statistics.median(times)
+    ref = gsb.Batch(plans, precision=gsb.GSB_C128)
+    ref.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+    lp128, ms128 = ref.run()
+    fin = np.isfinite(lp128)
+    d = np.abs(lp - lp128)[fin]
+    nstr = lp.size
+    # algorithmic bytes: per item one prefix sweep plus nsuf suffix sweeps (one write pass per step), the
+    # snapshot and its restores
+    E = 8
+    byt = 0
+    for w, K in zip(bw["instances"], bw["K"]):
+        st = w["steps"]
+        pre = sum((1 << s["r"]) + (1 << s["rn"]) for s in st[:K])
+        suf = sum((1 << s["r"]) + (1 << s["rn"]) for s in st[K:])
+        snap = 1 << st[K]["r"]
+        byt += 16 * E * (pre + 4 * suf + 2 * snap + 3 * 2 * snap)
+    peak, kind = peaks()
+    _form_line("batch", "amps/s, 512 instances n in [16,40] x 64 strings, one persistent launch", nstr / (ms / 1e3),
+               "amps/s", True, {
+                   "ms_per_launch": ms, "strings": int(nstr), "instances": len(plans),
+                   "widths": {"min": int(min(widths)), "max": int(max(widths)), "mean": float(np.mean(widths))},
+                   "dtype": "c64 arena, f32 sums, f64 norms/scales", "shape": {"block": block, "small_R": small_R,
+                                                                                 "ctas_per_sm": per_sm},
+                   "c128": {"ms_per_launch": ms128, "max_abs_dlog2p_c64_vs_c128": float(d.max()),
+                            "median_abs_dlog2p": float(np.median(d))},
+                   "roofline": {"bound": "hbm", "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
+                                "note": "team tables <= 2^20 entries: many items are L2-resident"},
+                   "host_planning_s": t_plan, "steps": args.steps, "warmup": args.warmup,
+               })
+
+
+def run_form_grad(args):
+    """Gradient of -mean log2 Pr over 2048 exact targets w.r.t. the 48 x 3 rotation angles (adjoint sweep)."""
+    import math
+    import numpy as np
+    import torch
+    import adjoint
+    import gsb
+    import workloads
+    w = workloads.rotation_instance(48, 48, seed=7, order_seed=12, iters=20000)
+    w2 = workloads.matching_instance(48, 48, 8, 12, 20000)
+    with gsb.Engine.from_text(w2["plan"], precision=gsb.GSB_C128) as eng2:
+        tb, _ = eng2.sample(2048, seed=99)
+    v2 = [s["v"] for s in w2["steps"]]
+    q = np.zeros((len(tb), 48), np.int8)
+    q[:, v2] = tb                                       # targets by qubit
+    bits = np.ascontiguousarray(q[:, w["step_vertices"]])   # in this instance's step order
+    theta = torch.tensor(np.random.default_rng(5).uniform(0, 2 * math.pi, (48, 3)), requires_grad=True)
+    sweep = gsb.GradSweep(w["plan"], every=4)
+    times = []
+    for i in range(max(3, args.warmup) + args.steps):
+        theta.grad = None
+        t0 = time.perf_counter()
+        loss = -adjoint.log2_prob(theta, w["M0"], w["step_vertices"], bits, sweep).mean()
+        loss.backward()
+        if i >= max(3, args.warmup):
+            times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    _form_line("grad", "s per loss+gradient, n=48 rotation layer, 2048 exact targets", t, "s", False, {
+        "strings_per_s": len(bits) / t, "loss": loss.item(), "grad_norm": float(theta.grad.norm()),
+        "width": w["width"], "checkpoint_every": 4, "dtype": "c128 arena, f64",
+        "targets": "2048 exact samples of a second seeded n=48 instance (complex128 executor)",
+        "steps": args.steps, "warmup": max(3, args.warmup)})
+
+
+def run_form_wide34(args):
+    """n = 80, width 34 in complex64: 256 amplitudes and 16 exact samples on one GPU."""
+    import numpy as np
+    import torch
+    import gsb
+    import workloads
+    t0 = time.perf_counter()
+    w = workloads.wide34_instance()
+    t_plan = time.perf_counter() - t0
+    ns = len(w["steps"])
+    strings = workloads.random_strings(ns, 256, seed=2024)
+    with gsb.Engine.from_text(w["plan"], precision=gsb.GSB_C64) as eng:
+        stream = torch.cuda.Stream()
+        eng.set_stream(stream.cuda_stream)
+        eng.chain(strings[:1])
+        t1 = time.perf_counter()
+        lp, _ = eng.chain(strings)
+        t_amp = time.perf_counter() - t1
+        t2 = time.perf_counter()
+        sbits, slp = eng.sample(16, seed=7)
+        t_smp = time.perf_counter() - t2
+    _form_line("wide34", "amps/s and s/sample at n=80, width 34, complex64 (137 GB arena)", 256 / t_amp, "amps/s", True, {
+        "s_per_sample": t_smp / 16, "width": w["width"], "arena_gb": (1 << w["width"]) * 8 / 1e9,
+        "log2p_first": [float(x) for x in lp[:4]], "sample_log2p": [float(x) for x in slp[:4]],
+        "dtype": "c64 arena, f32 sums, f64 norms/scales", "host_planning_s": t_plan,
+        "timing": "wall clock around the host-buffer C-ABI calls (whole batches, one synchronisation each)"})
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.profile_chain:
+    if a.form == "batch":
+        run_form_batch(a)
+    elif a.form == "grad":
+        run_form_grad(a)
+    elif a.form == "wide34":
+        run_form_wide34(a)
+    elif a.profile_chain:
         profile_chain(a)
     elif a.impl == "reference":
         run_reference(a)

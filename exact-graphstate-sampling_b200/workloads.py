@@ -66,6 +66,17 @@ def batch_workload(count=512, seed=0, nmin=16, nmax=40, npre=16, nsuf=4, iters=5
     return dict(instances=inst, K=K, prefixes=pre, suffixes=suf)
 
 
+def wide34_instance():
+    """The largest single-GPU width: n = 80, depth 80, circuit seed 6, order from the native search (seed 12, 8 greedy
+    starts, 60000 moves) of width 34: a 2^34-entry arena, 137 GB complex64."""
+    n, body, tail = circuits.matching_circuit(80, 80, seed=6)
+    from graphform import graph_form
+    A, _ = graph_form(circuits.tableau_of(n, body))
+    order, w = gsb.order_search(A, seed=12, ngreedy=8, iters=60000)
+    text, st, R = build(n, body, tail, order)
+    return dict(name="matching_n80_d80_s6_w34", n=n, body=body, tail=tail, order=order, width=R, plan=text, steps=st)
+
+
 def matching_n70_w30():
     return matching_instance(70, 70, 2, 12, 60000)
 
