@@ -46,6 +46,7 @@ import replicas  # noqa: E402  (package module: torchrun rank bookkeeping)
 
 METRIC = "s/sample & amps/s at n=70 w=30, c64 form vs c128 plain, |Δlog2P|≤1e-5; HBM GB/s"
 WORKLOAD = "matching_n70_d70_s2_w30"
+K_GROUP_TRAFFIC_RATIO = 0.9734
 
 
 def parse():
@@ -294,16 +295,18 @@ def run_gsb(args):
     fused = [k for k in range(ns) if glen[k] >= 2]
     fused_bytes = float(sum(gent[k] for k in fused)) * 8
     fused_ms = float(sum(wmean[k] for k in fused))
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "write_pass_traffic.json")
-    if os.path.exists(tpath):
-        traffic = json.load(open(tpath)).get("dram_bytes_per_string_c64")
-    # exact-sample passes (look-ahead norm + write per fused pair), per pass
+    # DRAM bytes per algorithmic byte of the dominant pass, from one ncu capture of k_group<float2, float, 2, 0> on the
+    # width-27 instance (2.0903 GB read + written for 2.1475 GB algorithmic: no re-reads; writes still dirty in L2
+    # at kernel end make it < 1), scaled to the chain passes of one string
+    traffic = pass_bytes * K_GROUP_TRAFFIC_RATIO
+    # exact-sample passes (a norm pass where a pass has no other source for its first bit, then the pass)
     sw, sn = eng.profile_steps(strings[0], mode=1)
     sample_kernel_ms = float(sw.sum() + sn.sum())
     sample_bytes = float(sum((2 * (1 << st["r"]) + (1 << st["rn"])) for st in steps)) * 8
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
-                "traffic": traffic, "peak_kind": peak_kind,
+                "traffic": traffic, "traffic_source": "ncu dram bytes of one k_group launch (width-27 capture) per "
+                                                      "algorithmic byte, times the pass bytes of one string",
+                "peak_kind": peak_kind,
                 "kernel": "chain passes: k_group<float2,float,*> (fused) + k_pair64/k_step (single steps)",
                 "pass_bytes_per_string": pass_bytes, "kernel_ms_per_string": kernel_ms,
                 "fused_passes_frac": (fused_bytes / (fused_ms / 1000.0) / 1e9) / hbm_peak if fused_ms > 0 else None,
