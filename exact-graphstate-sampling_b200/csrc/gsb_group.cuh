@@ -207,8 +207,8 @@ enum { GK_ANY = 0, GK_1_0, GK_2_0, GK_2_1, GK_4_0, GK_4_1, GK_4_2 };
 // Per coset: the x = 0 terms sum into their output, the x = 1 terms sum with the sign (-1)^par_t into theirs, and
 // output tau = M[b][0] * x0-sum + s * M[b][1] * x1-sum with the class sign s = (-1)^(parity(base & lambda) ^ mpar_j)
 // (gsamp2.cpp:32-38 with the sign parity(c & rhoc) ^ par of the reference's term list factored per class).
-// NB input tables (1, or 2 for the look-ahead's two branches of the previous step) are each rotated by NR rows of M
-// (1 for a write pass, 2 for the look-ahead's branch norms); nsum[b][r] gets the squares of table b under row r.
+// NB input tables (1, or 2 when both branches of the previous step are kept) are each rotated by NR rows of M
+// (1 for a written step, 2 for a trailing step's branch norms); nsum[b][r] gets the squares of table b under row r.
 // FIRST reads the tile's copy of the arena blocks (type E, class p of offset z at [z index][p ^ (z & mask)]), LAST
 // writes the arena (NB = NR = 1; class p of output offset z at TB ^ (z & ~mask) ^ p ^ (z & mask)), the other stages
 // use buffers [value index][class] of type CplxOf<T>; STS stores every (table, row) to such a buffer.  Buffers are

@@ -151,7 +151,8 @@ def test_statevector_n24():
 @pytest.mark.parametrize("mode", MODES)
 def test_fused_chain_depths_vs_oracle(wide_case, mode):
     """'chain' mode with 1, 2 and 3 DP steps fused per pass gives the oracle's log2 Pr and conditionals; 'prob' and
-    'sample' (pairs with a look-ahead norm pass) give the oracle's probabilities and bit-identical samples."""
+    'sample' (fused passes that carry the next step's branch norms) give the oracle's probabilities and
+    bit-identical samples."""
     import workloads
     from oracle import Oracle
     ns = n = len(wide_case["steps"])
@@ -170,7 +171,7 @@ def test_fused_chain_depths_vs_oracle(wide_case, mode):
                 assert abs(lp[i] - olp) <= lp_tol(mode, olp, n), (depth, i, lp[i], olp)
                 if olp > -n - 3:
                     assert np.abs(cond[i] - ocond).max() <= cond_tol(mode), depth
-            # 'prob' and 'sample' run pairs of steps with a look-ahead norm pass when fusion is on
+            # 'prob' and 'sample' run fused passes with trailing branch norms when fusion is on
             lpp = eng.prob(strings[:4])
             for i in range(4):
                 assert abs(lpp[i] - ref[i][0]) <= lp_tol(mode, ref[i][0], n), (depth, i)
