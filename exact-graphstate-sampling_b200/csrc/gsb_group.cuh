@@ -172,9 +172,12 @@ __device__ __forceinline__ void st_perm(double2 *m, uint32_t pos, const double (
 // shared memory [index][class]: P consecutive values
 template <int P>
 __device__ __forceinline__ void lds_cls(const float2 *q, float (&r)[P], float (&i)[P]) {
-    if (P == 2) {
-        const float4 v = *reinterpret_cast<const float4 *>(q);
-        r[0] = v.x; i[0] = v.y; r[P - 1] = v.z; i[P - 1] = v.w;
+    if (P >= 2) {
+#pragma unroll
+        for (int c = 0; c < P; c += 2) {
+            const float4 v = *reinterpret_cast<const float4 *>(q + c);
+            r[c] = v.x; i[c] = v.y; r[c + 1] = v.z; i[c + 1] = v.w;
+        }
     } else {
         r[0] = q[0].x; i[0] = q[0].y;
     }
@@ -186,8 +189,12 @@ __device__ __forceinline__ void lds_cls(const double2 *q, double (&r)[P], double
 }
 template <int P>
 __device__ __forceinline__ void sts_cls(float2 *q, const float (&r)[P], const float (&i)[P]) {
-    if (P == 2) *reinterpret_cast<float4 *>(q) = make_float4(r[0], i[0], r[P - 1], i[P - 1]);
-    else q[0] = make_float2(r[0], i[0]);
+    if (P >= 2) {
+#pragma unroll
+        for (int c = 0; c < P; c += 2) *reinterpret_cast<float4 *>(q + c) = make_float4(r[c], i[c], r[c + 1], i[c + 1]);
+    } else {
+        q[0] = make_float2(r[0], i[0]);
+    }
 }
 template <int P>
 __device__ __forceinline__ void sts_cls(double2 *q, const double (&r)[P], const double (&i)[P]) {
@@ -222,7 +229,7 @@ __device__ __forceinline__ void group_cosets(const GroupArgs &ga, const GroupSte
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr bool ANY = H < 0;
     const uint32_t NC = 1u << L;
-    const int LG = P == 2 ? L - 1 : L;                 // log2 class groups per tile
+    const int LG = L - (P == 4 ? 2 : P == 2 ? 1 : 0);  // log2 class groups per tile
     const uint32_t NG = 1u << LG;
     const int tpar = __popcll(TB & gs.lambda) & 1;
     const int nm = gs.nmem;
@@ -304,7 +311,7 @@ __device__ __forceinline__ void group_cosets(const GroupArgs &ga, const GroupSte
             T w1r[NR][P], w1i[NR][P];
 #pragma unroll
             for (int c = 0; c < P; c++) {
-                const bool neg = ((mp ^ __popc((pc + c) & lam)) & 1) != 0;
+                const bool neg = ((mp ^ __popc(pc & lam) ^ __popc((uint32_t)c & lam)) & 1) != 0;   // pc: multiple of P
 #pragma unroll
                 for (int r = 0; r < NR; r++) {
                     w1r[r][c] = neg ? -w_r[r][1] : w_r[r][1];
@@ -357,7 +364,10 @@ __device__ __forceinline__ void group_cosets_any(const GroupArgs &ga, const Grou
                                                  const uint64_t TB, const int L, const uint32_t (&in)[NB],
                                                  const uint32_t (&out)[NB][NR], const T (&w_r)[NR][2],
                                                  const T (&w_i)[NR][2], T (&ns)[NB][NR]) {
-    constexpr int P = sizeof(E) == 8 ? 2 : 1;          // complex64: a thread takes two adjacent classes
+    // classes per thread: two adjacent classes for complex64 (their values sit in one 16-byte span of a block),
+    // one for complex128.  Four per thread was measured slower: per-class 8-byte accesses at a 32-byte stride
+    // conflict in shared memory and scatter the arena stores.
+    constexpr int P = sizeof(E) == 8 ? 2 : 1;
 #define GSB_GC(NTQ_, H_) group_cosets<E, T, P, NTQ_, H_, FIRST, LAST, STS, NB, NR>(ga, gs, mem, TB, L, in, out, w_r, w_i, ns)
     switch (gs.kind) {   // uniform across the grid
         case GK_1_0: GSB_GC(1, 0); break;
@@ -493,8 +503,10 @@ __host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L) {
 // buffer n & 1 (completion on that buffer's mbarrier) two tiles ahead: the loads of tile n + 2 are issued as soon as
 // tile n's first step has read its buffer.  The last written step stores straight to the arena.  A tile's writes
 // never reach another class's input (checked on the host), so the early loads are race-free.
+// Two CTAs per SM (the shared-memory budget allows no more), so up to 128 registers a thread: without this bound the
+// compiler kept some instantiations at 64-80 registers and spilled.
 template <typename E, typename T, int D, int TR>
-__global__ void __launch_bounds__(256) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
+__global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
     DevState *st = cx.st;
     if (*(volatile int *)&st->dead) return;
     extern __shared__ __align__(16) unsigned char smem[];
