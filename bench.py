@@ -492,11 +492,36 @@ def run_form_wide34(args):
         t2 = time.perf_counter()
         sbits, slp = eng.sample(16, seed=7)
         t_smp = time.perf_counter() - t2
+    # complex128 cross-check of 4 amplitudes: a second order with 3 slice vertices cut out (width 33), every slice's
+    # final table from 'prefix', summed by 'resume' (the reference's slicing identity)
+    t3 = time.perf_counter()
+    sl = workloads.wide34_slices(w)
+    v1 = [s["v"] for s in w["steps"]]
+    check = []
+    with gsb.Engine.from_text(sl["plans"][0], precision=gsb.GSB_C128) as e128:
+        ns2 = e128.ns
+        for i in range(4):
+            q = np.zeros(w["n"], np.int8)
+            q[v1] = strings[i]
+            line = q[sl["step_vertices"]]
+            dumps, lss = [], []
+            for text in sl["plans"]:
+                e128.set_matrices_from_text(text)
+                d, ls, _ = e128.prefix(line, ns2)
+                dumps.append(d)
+                lss.append(ls)
+            _, lpf, _, _ = e128.resume(line, ns2, 0, 0, dumps, lss)
+            check.append((float(lp[i]), float(lpf)))
+    t_check = time.perf_counter() - t3
     _form_line("wide34", "amps/s and s/sample at n=80, width 34, complex64 (137 GB arena)", 256 / t_amp, "amps/s", True, {
         "s_per_sample": t_smp / 16, "width": w["width"], "arena_gb": (1 << w["width"]) * 8 / 1e9,
         "log2p_first": [float(x) for x in lp[:4]], "sample_log2p": [float(x) for x in slp[:4]],
         "dtype": "c64 arena, f32 sums, f64 norms/scales", "host_planning_s": t_plan,
-        "timing": "wall clock around the host-buffer C-ABI calls (whole batches, one synchronisation each)"})
+        "timing": "wall clock around the host-buffer C-ABI calls (whole batches, one synchronisation each)",
+        "c128_sliced_check": {"slices": len(sl["plans"]), "slice_vertices": sl["S"], "width": sl["width"],
+                              "arena_gb": (1 << sl["width"]) * 16 / 1e9,
+                              "log2p_c64_vs_c128": check,
+                              "max_abs_dlog2p": max(abs(a - b) for a, b in check), "seconds": t_check}})
 
 
 if __name__ == "__main__":

@@ -77,6 +77,34 @@ def wide34_instance():
     return dict(name="matching_n80_d80_s6_w34", n=n, body=body, tail=tail, order=order, width=R, plan=text, steps=st)
 
 
+def wide34_slices(w, S=(0, 3, 2), order_seed=5, iters=60000):
+    """The width-34 instance's complex128 cross-check: a second order for the graph with the slice vertices S cut out
+    (native search, seed 5: width 33 for S = (0, 3, 2), so a 2^33-entry complex128 arena, 137 GB, fits), and the
+    reference-format slice plans of make_sliced_plans on it, one per assignment of S.  Every slice vertex and all of
+    their neighbours are eliminated by the last step, so the slices' final tables add up with no twist."""
+    import os
+    import tempfile
+    from graphform import graph_form
+    from sliced_plans import make_sliced_plans
+    n = w["n"]
+    T = circuits.tableau_of(n, w["body"])
+    A, _ = graph_form(T)
+    A = np.array(A, np.uint8)
+    A2 = A.copy()
+    for v in S:
+        A2[v, :] = 0
+        A2[:, v] = 0
+    order2, width2 = gsb.order_search(A2, seed=order_seed, ngreedy=4, iters=iters)
+    am = Amplitudes(n, T, w["tail"], order2)
+    with tempfile.TemporaryDirectory() as td:
+        out = os.path.join(td, "sl")
+        info = make_sliced_plans(A, [m.copy() for m in am.M], list(order2), list(S), out, ND=n)
+        plans = [open(f"{out}_s{''.join(map(str, bits))}.txt").read()
+                 for bits in np.ndindex(*([2] * len(S)))]
+    return dict(S=list(S), order=list(order2), width=info["R"], K=info["K"], twist=info["twist"], plans=plans,
+                step_vertices=info["step_vertices"])
+
+
 def matching_n70_w30():
     return matching_instance(70, 70, 2, 12, 60000)
 

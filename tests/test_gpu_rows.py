@@ -151,3 +151,34 @@ def _write_inputs(extras, d, tmp_path):
     for tag, text in sl["plans"].items():
         (tmp_path / f"sl_s{tag}.txt").write_text(text)
     (tmp_path / "sl_twist.txt").write_text(sl["twist"])
+
+
+def test_slices_summed_after_the_last_step(planner_cases, tmp_path):
+    """Slicing with every slice vertex's neighbours in the sweep (K = ns, no twist): 'prefix' through the last step
+    on every slice plan and 'resume' with no steps left give the unsliced log2 Pr (the width-34 cross-check's use)."""
+    import gsb
+    from inplace import inplace_plan_text, plan_inplace, plan_width
+    from sliced_plans import make_sliced_plans
+    case = [c for c in planner_cases["cases"] if c["n"] >= 10][0]
+    am, c = _am(planner_cases, case["name"])
+    n = c["n"]
+    S = [c["order"][1], c["order"][n // 2]]
+    out = str(tmp_path / "sp")
+    info = make_sliced_plans(am.A, [m.copy() for m in am.M], c["order"], S, out, ND=n)
+    assert info["K"] == n and not info["twist"]
+    R = max(1, plan_width(am.steps))
+    rng = np.random.default_rng(9)
+    with gsb.Engine.from_text(inplace_plan_text(plan_inplace(am.A, c["order"], R), R, am.M, n), precision=128) as full, \
+            gsb.Engine(f"{out}_s00.txt", precision=128) as e:
+        texts = [open(f"{out}_s{a}{b}.txt").read() for a in (0, 1) for b in (0, 1)]
+        for _ in range(5):
+            line = [int(x) for x in rng.integers(0, 2, n)]
+            dumps, lss = [], []
+            for t in texts:
+                e.set_matrices_from_text(t)
+                d, ls, _ = e.prefix(line, n)
+                dumps.append(d)
+                lss.append(ls)
+            _, lpf, _, _ = e.resume(line, n, 0, 0, dumps, lss)
+            ref = full.chain([line])[0][0]
+            assert abs(lpf - ref) <= 1e-9 or abs(2 ** lpf - 2 ** ref) <= 1e-12
