@@ -12,9 +12,10 @@
 // with lambda_ns = 1 at the final entry.  Each coset reads and writes only its own slots, so the reverse pass is
 // in place and race-free like the forward one.  The reverse pass needs T_k: the forward sweep keeps a compact copy
 // of the live table ([coset][offset], 2^{r_k} entries) every `every` steps, and each segment between two
-// checkpoints is recomputed forward once, keeping its tables, before the reverse pass walks it.  Per string the
-// whole sequence (forward, then per segment: restore, recompute, reverse) is one CUDA graph; the string index lives
-// in device memory and advances at its end.
+// checkpoints is recomputed forward once, keeping its tables, before the reverse pass walks it.  Up to 32 strings
+// are swept together (grid dimension y: each string owns its arenas, checkpoints, segment tables and reduction
+// slots), and the whole sequence of such a launch (forward, then per segment: restore, recompute, reverse) is one
+// CUDA graph; the first string's index lives in device memory and advances at its end.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -30,11 +31,13 @@
 
 namespace gsb {
 
+// A launch sweeps `bs` strings at once: string y = blockIdx.y is item *item + y and owns slot y of every buffer.
 struct GradCtx {
     const double *M;         // [ns][2][2] (re, im): the caller's matrices
     const int8_t *bits;      // [cap][ns]
-    const int *item;         // current string
-    int ns;
+    const int *item;         // first string of the launch
+    int ns, maxgrid;
+    size_t arena;            // entries per string: T and Lam arenas
 };
 
 __device__ __forceinline__ uint64_t coset_base(const StepArgs &s, uint64_t c) {
@@ -48,7 +51,7 @@ __device__ __forceinline__ uint64_t coset_base(const StepArgs &s, uint64_t c) {
 }
 
 __device__ __forceinline__ void step_row(const StepArgs &s, const GradCtx &g, double2 &m0, double2 &m1) {
-    const int b = g.bits[(size_t)*g.item * (size_t)g.ns + (size_t)s.k];
+    const int b = g.bits[(size_t)(*g.item + (int)blockIdx.y) * (size_t)g.ns + (size_t)s.k];
     const double *Mk = g.M + (size_t)s.k * 8 + 4 * b;
     m0 = make_double2(Mk[0], Mk[1]);
     m1 = make_double2(Mk[2], Mk[3]);
@@ -60,14 +63,16 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
 __device__ __forceinline__ double2 cadd(double2 a, double2 b) { return make_double2(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ double2 cscale(double s, double2 a) { return make_double2(s * a.x, s * a.y); }
 
-__global__ void k_gr_begin(double2 *T) { T[0] = make_double2(1.0, 0.0); }
+__global__ void k_gr_begin(double2 *T, const GradCtx g) { T[blockIdx.y * g.arena] = make_double2(1.0, 0.0); }
 
 // Forward step on the T arena: gathers the input table to `gather` ([c][t], if given) and, if `write`, stores the
 // step's outputs in place.
 __global__ void __launch_bounds__(256) k_gr_fwd(const StepArgs s, double2 *__restrict__ T, double2 *__restrict__ gather,
-                                                int write, const GradCtx g) {
+                                                size_t gather_stride, int write, const GradCtx g) {
     double2 m0, m1;
     step_row(s, g, m0, m1);
+    T += blockIdx.y * g.arena;
+    if (gather) gather += blockIdx.y * gather_stride;
     const uint64_t N = 1ULL << s.nk;
     for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t base = coset_base(s, c);
@@ -88,7 +93,10 @@ __global__ void __launch_bounds__(256) k_gr_fwd(const StepArgs s, double2 *__res
 }
 
 // Restore a checkpoint: the compact table [c][t] back to its arena slots.
-__global__ void __launch_bounds__(256) k_gr_scatter(const StepArgs s, const double2 *__restrict__ src, double2 *__restrict__ T) {
+__global__ void __launch_bounds__(256) k_gr_scatter(const StepArgs s, const double2 *__restrict__ src, size_t src_stride,
+                                                    double2 *__restrict__ T, const GradCtx g) {
+    src += blockIdx.y * src_stride;
+    T += blockIdx.y * g.arena;
     const uint64_t N = 1ULL << s.nk;
     for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t base = coset_base(s, c);
@@ -97,21 +105,26 @@ __global__ void __launch_bounds__(256) k_gr_scatter(const StepArgs s, const doub
 }
 
 // End of the forward sweep: Z = T[0]; lambda_ns = 1.
-__global__ void k_gr_final(const double2 *T, double2 *Lam, double2 *z_out, const int *item) {
-    z_out[*item] = T[0];
-    Lam[0] = make_double2(1.0, 0.0);
+__global__ void k_gr_final(const double2 *T, double2 *Lam, double2 *z_out, const GradCtx g) {
+    z_out[*g.item + (int)blockIdx.y] = T[blockIdx.y * g.arena];
+    Lam[blockIdx.y * g.arena] = make_double2(1.0, 0.0);
 }
 
-__global__ void k_gr_next(int *item) { *item += 1; }
+__global__ void k_gr_next(int *item, int bs) { *item += bs; }
 __global__ void k_gr_set_item(int *item, int v) { *item = v; }
 
 // Reverse step: lambda_{k+1} (output slots of the Lam arena) -> lambda_k (input slots, in place), and
 // dZ/dM_k[b_k][x] from the step's input table Tk ([c][t]).  Deterministic reduction: per-block partials, the last
 // block sums them in block order and writes grad[item][k] = (dZ/dm0, dZ/dm1).
-__global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 *__restrict__ Tk, double2 *__restrict__ Lam,
-                                                const GradCtx g, double *partials, unsigned int *counter, double *grad) {
+__global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 *__restrict__ Tk, size_t tk_stride,
+                                                double2 *__restrict__ Lam, const GradCtx g, double *partials,
+                                                unsigned int *counter, double *grad) {
     double2 m0, m1;
     step_row(s, g, m0, m1);
+    Tk += blockIdx.y * tk_stride;
+    Lam += blockIdx.y * g.arena;
+    partials += (size_t)blockIdx.y * 4 * (size_t)g.maxgrid;
+    counter += blockIdx.y;
     const uint64_t N = 1ULL << s.nk;
     double a[4] = {0, 0, 0, 0};   // dZ/dm0 (re, im), dZ/dm1 (re, im)
     for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
@@ -154,16 +167,17 @@ __global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 
     double t[4] = {0, 0, 0, 0};
     for (unsigned int b = 0; b < gridDim.x; b++)
         for (int i = 0; i < 4; i++) t[i] += __ldcg(partials + 4 * b + i);
-    double *out = grad + ((size_t)*g.item * (size_t)g.ns + (size_t)s.k) * 4;
+    double *out = grad + ((size_t)(*g.item + (int)blockIdx.y) * (size_t)g.ns + (size_t)s.k) * 4;
     for (int i = 0; i < 4; i++) out[i] = t[i];
     *counter = 0;
 }
 
 struct GradEngine {
     HPlan plan;
-    int dev = 0, sms = 0, every = 4, cap = 1024;
+    int dev = 0, sms = 0, every = 4, cap = 1024, bs = 1;   // cap: strings per host batch, a multiple of bs
     std::vector<StepArgs> args;
-    std::vector<size_t> ckpt_off;      // offset (entries) of step k's checkpoint in d_ckpt (k % every == 0)
+    std::vector<size_t> ckpt_off;      // offset (entries) of step k's checkpoint in a string's checkpoint slot
+    size_t arena = 0, ckpt_n = 0;      // entries per string: arena, checkpoints
     double2 *T = nullptr, *Lam = nullptr, *d_ckpt = nullptr, *d_seg = nullptr;
     size_t seg_stride = 0;             // entries per segment table
     double *d_M = nullptr, *partials = nullptr, *d_grad = nullptr;
@@ -195,39 +209,44 @@ struct GradEngine {
         cudaSetDevice(prev);
     }
 
-    int grid_of(const StepArgs &s) const {
+    dim3 grid_of(const StepArgs &s) const {
         const uint64_t N = 1ULL << s.nk;
-        return (int)std::max<uint64_t>(1, std::min<uint64_t>((N + 255) / 256, (uint64_t)maxgrid));
+        return dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((N + 255) / 256, (uint64_t)maxgrid)), (unsigned)bs);
     }
-    GradCtx ctx() const { return GradCtx{d_M, d_bits, d_item, plan.ns}; }
-    double2 *seg(int pos) const { return d_seg + (size_t)(pos - 1) * seg_stride; }   // pos = 1 .. every-1
+    GradCtx ctx() const { return GradCtx{d_M, d_bits, d_item, plan.ns, maxgrid, arena}; }
+    size_t seg_per_string() const { return (size_t)std::max(0, every - 1) * seg_stride; }
+    double2 *seg(int pos) const { return d_seg + (size_t)(pos - 1) * seg_stride; }   // pos = 1 .. every-1 (slot 0)
 
-    // The per-string sequence (captured once as a graph).
+    // The sequence of one launch of bs strings (captured once as a graph).
     cudaError_t enqueue() {
         const int ns = plan.ns;
         const GradCtx g = ctx();
-        k_gr_begin<<<1, 1, 0, stream>>>(T);
+        const dim3 one(1, (unsigned)bs);
+        k_gr_begin<<<one, 1, 0, stream>>>(T, g);
         for (int k = 0; k < ns; k++) {
             const StepArgs &s = args[(size_t)k];
-            k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, k % every == 0 ? d_ckpt + ckpt_off[(size_t)k] : nullptr, 1, g);
+            k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, k % every == 0 ? d_ckpt + ckpt_off[(size_t)k] : nullptr,
+                                                    ckpt_n, 1, g);
         }
-        k_gr_final<<<1, 1, 0, stream>>>(T, Lam, d_z, d_item);
+        k_gr_final<<<one, 1, 0, stream>>>(T, Lam, d_z, g);
         for (int c = ((ns - 1) / every) * every; c >= 0; c -= every) {
             const int e = std::min(c + every, ns);
             const StepArgs &sc = args[(size_t)c];
-            k_gr_scatter<<<grid_of(sc), 256, 0, stream>>>(sc, d_ckpt + ckpt_off[(size_t)c], T);
+            k_gr_scatter<<<grid_of(sc), 256, 0, stream>>>(sc, d_ckpt + ckpt_off[(size_t)c], ckpt_n, T, g);
             for (int j = c; j < e; j++) {   // recompute: gather T_j (j > c), write T_{j+1} (j < e - 1)
                 if (j == c && e - 1 == c) break;
                 const StepArgs &s = args[(size_t)j];
-                k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, j == c ? nullptr : seg(j - c), j < e - 1 ? 1 : 0, g);
+                k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, j == c ? nullptr : seg(j - c), seg_per_string(),
+                                                        j < e - 1 ? 1 : 0, g);
             }
             for (int j = e - 1; j >= c; j--) {
                 const StepArgs &s = args[(size_t)j];
                 const double2 *tk = j == c ? d_ckpt + ckpt_off[(size_t)c] : seg(j - c);
-                k_gr_bwd<<<grid_of(s), 256, 0, stream>>>(s, tk, Lam, g, partials, d_counter, d_grad);
+                k_gr_bwd<<<grid_of(s), 256, 0, stream>>>(s, tk, j == c ? ckpt_n : seg_per_string(), Lam, g, partials,
+                                                        d_counter, d_grad);
             }
         }
-        k_gr_next<<<1, 1, 0, stream>>>(d_item);
+        k_gr_next<<<1, 1, 0, stream>>>(d_item, bs);
         return cudaGetLastError();
     }
 };
@@ -314,30 +333,38 @@ int gsb_grad_open_text(const char *text, size_t len, int device, int every, gsb_
         }
     }
     E.seg_stride = maxr;
+    E.ckpt_n = ck;
     const size_t arena = (size_t)1 << p.R;
+    E.arena = arena;
     size_t free_b = 0, total_b = 0;
     cudaMemGetInfo(&free_b, &total_b);
-    const size_t need = 16 * (2 * arena + ck + (size_t)std::max(0, every - 1) * maxr);
-    if (need > free_b / 10 * 9) {
+    // strings per launch: a power of two up to 32, each with its own arenas, checkpoints and segment tables, within
+    // half of the free device memory
+    const size_t per_string = 16 * (2 * arena + ck + (size_t)std::max(0, every - 1) * maxr) +
+                              (size_t)E.maxgrid * 4 * sizeof(double);
+    if (per_string > free_b / 10 * 9) {
         delete h;
-        return fail(GSB_E_ALLOC, "arena, checkpoints and segment tables need " + std::to_string(need) +
+        return fail(GSB_E_ALLOC, "arena, checkpoints and segment tables need " + std::to_string(per_string) +
                                      " bytes; the device has " + std::to_string(free_b) + " free");
     }
+    E.bs = 1;
+    while (E.bs < 32 && (size_t)(2 * E.bs) * per_string <= free_b / 2) E.bs *= 2;
+    const size_t bs = (size_t)E.bs;
     cudaError_t e = cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMalloc(&E.T, arena * 16);
-    if (e == cudaSuccess) e = cudaMalloc(&E.Lam, arena * 16);
-    if (e == cudaSuccess) e = cudaMalloc(&E.d_ckpt, std::max<size_t>(ck, 1) * 16);
-    if (e == cudaSuccess) e = cudaMalloc(&E.d_seg, std::max<size_t>((size_t)std::max(0, every - 1) * maxr, 1) * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.T, bs * arena * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.Lam, bs * arena * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_ckpt, bs * std::max<size_t>(ck, 1) * 16);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_seg, bs * std::max<size_t>(E.seg_per_string(), 1) * 16);
     if (e == cudaSuccess) e = cudaMalloc(&E.d_M, (size_t)p.ns * 8 * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&E.partials, (size_t)E.maxgrid * 4 * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&E.partials, bs * (size_t)E.maxgrid * 4 * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&E.d_grad, (size_t)E.cap * (size_t)p.ns * 4 * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&E.d_z, (size_t)E.cap * sizeof(double2));
     if (e == cudaSuccess) e = cudaMalloc(&E.d_bits, (size_t)E.cap * (size_t)p.ns);
     if (e == cudaSuccess) e = cudaMalloc(&E.d_item, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&E.d_counter, sizeof(unsigned int));
-    if (e == cudaSuccess) e = cudaMemsetAsync(E.d_counter, 0, sizeof(unsigned int), E.stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(E.T, 0, arena * 16, E.stream);
-    if (e == cudaSuccess) e = cudaMemsetAsync(E.Lam, 0, arena * 16, E.stream);
+    if (e == cudaSuccess) e = cudaMalloc(&E.d_counter, bs * sizeof(unsigned int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(E.d_counter, 0, bs * sizeof(unsigned int), E.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(E.T, 0, bs * arena * 16, E.stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(E.Lam, 0, bs * arena * 16, E.stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(E.stream);
     if (e != cudaSuccess) {
         delete h;
@@ -383,10 +410,13 @@ int gsb_grad_run(gsb_grad *h, const double *M, const int8_t *bits, int64_t nstr,
     }
     for (int64_t off = 0; off < nstr; off += E.cap) {
         const int64_t nb = std::min<int64_t>(E.cap, nstr - off);
+        const int64_t launches = (nb + E.bs - 1) / E.bs;   // the last launch's unused slots run all-zero strings
         GR_CK(cudaMemcpyAsync(E.d_bits, bits + off * ns, (size_t)(nb * ns), cudaMemcpyHostToDevice, E.stream));
+        if (launches * E.bs > nb)
+            GR_CK(cudaMemsetAsync(E.d_bits + nb * ns, 0, (size_t)((launches * E.bs - nb) * ns), E.stream));
         k_gr_set_item<<<1, 1, 0, E.stream>>>(E.d_item, 0);
         GR_CK(cudaGetLastError());
-        for (int64_t i = 0; i < nb; i++) GR_CK(cudaGraphLaunch(E.graph, E.stream));
+        for (int64_t i = 0; i < launches; i++) GR_CK(cudaGraphLaunch(E.graph, E.stream));
         GR_CK(cudaMemcpyAsync(z + 2 * off, E.d_z, (size_t)nb * 16, cudaMemcpyDeviceToHost, E.stream));
         GR_CK(cudaMemcpyAsync(dz + off * ns * 4, E.d_grad, (size_t)(nb * ns) * 4 * sizeof(double),
                               cudaMemcpyDeviceToHost, E.stream));
