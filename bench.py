@@ -12,9 +12,9 @@ One step = the exact amplitudes (log2 Pr and all 70 conditionals, 'chain' mode: 
 --amps-per-step uniform random bitstrings in the complex64 form.  `value` is amplitudes/s with the strings already
 in HBM (device-resident entry point), timed with CUDA events on the engine's stream, max over ranks; `e2e` is the
 same metric through the host-buffer C-ABI call (strings copied in from pinned host memory, log2 Pr and
-conditionals copied back, every step).  Extra keys report exact samples (s/sample, two passes per DP step), the
-complex128 form, the complex64-vs-complex128 agreement, the roofline of the dominant kernel and the reference's CPU
-executor timed on this host.
+conditionals copied back, every step).  Extra keys report exact samples (s/sample), the complex128 form (with the
+same fused passes, and its samples also with one norm and one write pass per step), the complex64-vs-complex128
+agreement, the roofline of the dominant kernel and the reference's CPU executor timed on this host.
 
 Multi-GPU: replicas only (the arena sweep does not shard without an all-to-all per step): each rank evaluates its
 own strings on its own GPU; value = all ranks' amplitudes / the slowest rank's time.
@@ -338,15 +338,26 @@ def run_gsb(args):
         dlp = float(np.abs(lp128 - lp64[sl]).max())
         dcond = float(np.abs(d_cond128.cpu().numpy() - cond64[sl]).max())
         S2 = args.c128_samples
-        e0.record(stream)
-        e128.sample_device(d_u[:S2], d_sb[:S2], d_slp[:S2])
-        e1.record(stream)
-        torch.cuda.synchronize()
-        s_per_sample128 = e0.elapsed_time(e1) / 1000.0 / S2
+
+        def time_samples128():
+            e128.sample_device(d_u[:1], d_sb[:1], d_slp[:1])      # graph built outside the timed region
+            torch.cuda.synchronize()
+            e0.record(stream)
+            e128.sample_device(d_u[:S2], d_sb[:S2], d_slp[:S2])
+            e1.record(stream)
+            torch.cuda.synchronize()
+            return e0.elapsed_time(e1) / 1000.0 / S2
+
+        s_per_sample128 = time_samples128()
         same_bits = bool((d_sb[:S2].cpu().numpy() == sbits64[:S2]).all())
+        # the same complex128 form without fusion: one norm pass and one write pass per DP step, the structure of
+        # the reference executor's two-pass sampler (gsamp2.cpp:39-55)
+        e128.set_fusion(1)
+        s_per_sample128_unfused = time_samples128()
         e128.close()
         c128 = {"amps_per_s": amps128,
-                "s_per_sample": s_per_sample128, "max_abs_dlog2p_c64_vs_c128": dlp,
+                "s_per_sample": s_per_sample128, "s_per_sample_unfused_two_pass": s_per_sample128_unfused,
+                "max_abs_dlog2p_c64_vs_c128": dlp,
                 "max_abs_dcond_c64_vs_c128": dcond, "samples_same_bits_c64_c128": same_bits}
 
     # per string: begin + one launch per chain pass + finish; one item reset per batch
