@@ -95,6 +95,8 @@ __device__ __forceinline__ void ld_e(const float2 *m, uint64_t a, float &r, floa
 __device__ __forceinline__ void ld_e(const double2 *m, uint64_t a, double &r, double &i) { const double2 v = m[a]; r = v.x; i = v.y; }
 __device__ __forceinline__ void st_e(float2 *m, uint64_t a, float r, float i) { m[a] = make_float2(r, i); }
 __device__ __forceinline__ void st_e(double2 *m, uint64_t a, double r, double i) { m[a] = make_double2(r, i); }
+__device__ __forceinline__ void ld_e(const float2 *m, uint64_t a, double &r, double &i) { const float2 v = m[a]; r = v.x; i = v.y; }
+__device__ __forceinline__ void st_e(float2 *m, uint64_t a, double r, double i) { m[a] = make_float2((float)r, (float)i); }
 
 __device__ __forceinline__ uint64_t bcoset_base(const uint64_t *tk, uint64_t c) {
     uint64_t b = 0;
@@ -178,7 +180,7 @@ __device__ void run_item(const TM &tm, const BatchArgs &a, int item, E *arena, E
     const BInst in = a.inst[ii];
     const BStep *st = a.steps + in.step_off;
     const int8_t *pb = a.pre_bits + in.pre_off + (int64_t)pre * in.K;
-    if (tm.rank() == 0) st_e(arena, 0, 1, 0);
+    if (tm.rank() == 0) st_e(arena, 0, 1.0, 0.0);
     tm.sync();
     ChainState cs{1.0, 0.0, 1.0, 0, 0};
     for (int k = 0; k < in.K && !cs.dead; k++) chain_update(cs, team_step(tm, st[k], a.tk + st[k].tk_off, arena, pb[k], cs.scale));
