@@ -73,6 +73,8 @@ def parse():
     ap.add_argument("--form", default="headline", choices=["headline", "batch", "grad", "wide34"],
                     help="workload to measure (the default line is the headline n = 70, width-30 workload)")
     ap.add_argument("--batch-instances", type=int, default=512)
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the byte-model pass lists (skip the guarded autotuner)")
     return ap.parse_args()
 
 
@@ -217,6 +219,8 @@ def run_gsb(args):
     eng = gsb.Engine.from_text(w["plan"], precision=64, device=local)
     eng.set_arith(args.arith)
     eng.set_fusion(args.fusion)
+    # guarded autotuner of the pass lists (kept only where a whole item gets faster), outside every timed region
+    tune64 = eng.autotune(mode=2, reps=3) if args.autotune else None
     stream = torch.cuda.Stream()                  # a real stream: the engine's kernels and the events share it
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
@@ -322,6 +326,7 @@ def run_gsb(args):
     if args.c128_amps > 0:
         e128 = gsb.Engine.from_text(w["plan"], precision=128, device=local)
         e128.set_fusion(args.fusion)
+        tune128 = e128.autotune(mode=2, reps=3) if args.autotune else None
         e128.set_stream(stream.cuda_stream)
         B = args.c128_amps
         d_lp128 = torch.empty(B, dtype=torch.float64, device="cuda")
@@ -355,7 +360,7 @@ def run_gsb(args):
         e128.set_fusion(1)
         s_per_sample128_unfused = time_samples128()
         e128.close()
-        c128 = {"amps_per_s": amps128,
+        c128 = {"amps_per_s": amps128, "autotune_ms_item_before_after": tune128,
                 "s_per_sample": s_per_sample128, "s_per_sample_unfused_two_pass": s_per_sample128_unfused,
                 "max_abs_dlog2p_c64_vs_c128": dlp,
                 "max_abs_dcond_c64_vs_c128": dcond, "samples_same_bits_c64_c128": same_bits}
@@ -370,6 +375,7 @@ def run_gsb(args):
                    "arith": args.arith, "fusion": args.fusion, "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
         "s_per_sample": s_per_sample64, "samples_per_s": world / s_per_sample64,
         "c128": c128, "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
+        "autotune_ms_item_before_after": tune64,
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -112,7 +112,7 @@ static void *pick_group(int d, int tr) {
 // One pass of an item: a single step (group == false: norm pass + write pass when sampling) or a fused group that
 // writes d steps and, with tr = 1, evaluates the next step's branch norms (sampling only).
 struct Op {
-    int k0 = 0, d = 1, tr = 0;
+    int k0 = 0, d = 1, tr = 0, lcap = 0;   // lcap: the tile-size cap the pass was built with (fused passes)
     bool group = false;
     bool norm_first = false;  // sampling: a norm pass of step k0 runs first (its bit has no other source)
     GroupArgs ga;
@@ -134,6 +134,12 @@ constexpr uint32_t GROUP_SMEM_PREF = GSB_GROUP_SMEM_PREF;   // tiles are shrunk 
 constexpr int GROUP_MAX_L = GSB_GROUP_MAX_L;                // at most 2^GROUP_MAX_L classes per tile
 constexpr int GROUP_MIN_R = 12;                     // steps below 2^12 entries run unfused
 
+// What a pass is, without its arguments: rebuilt with the current matrices whenever they change.
+struct OpShape {
+    int k0 = 0, d = 1, tr = 0, lcap = 0, src = 0;
+    bool group = false, norm_first = false;
+};
+
 template <typename E, typename T>
 static uint32_t group_smem_bytes(int D, int TR, const int (&ssz)[4], int L) {
     if (TR) return D == 2 ? group_smem<E, T, 2, 1>(ssz, L).total : group_smem<E, T, 1, 1>(ssz, L).total;
@@ -147,6 +153,8 @@ struct Engine {
     int fuse_depth = 2;                  // chain mode: largest number of DP steps fused into one pass (1 = none)
     std::vector<Op> chain_ops;           // 'chain' passes
     std::vector<Op> sample_ops;          // 'prob' / 'sample' passes (build_sample_ops)
+    std::vector<OpShape> chain_shapes;   // pass lists chosen by gsb_autotune (empty: the byte-model defaults)
+    std::vector<OpShape> sample_shapes;
     size_t esize = 8;
     void *mem = nullptr;
     cudaStream_t stream = nullptr;       // where work is queued (own_stream unless the caller set one)
@@ -383,7 +391,7 @@ static bool analytic_step(const HStep &hs) {
 
 // Group arguments of a fused pass from the host derivation and the steps' descriptors.  The pass writes stage gp.ws;
 // with gp.ws = gp.d - 1 the last step is the trailing norm step.
-static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
+static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_MAX_L) {
     const HPlan &p = E.plan;
     const int D = gp.ws, TR = gp.d - gp.ws;
     if (gp.stage_size[0] > 32 || gp.stage_size[D] > 32) return false;
@@ -394,7 +402,7 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
         if (E.arith == 64) return group_smem_bytes<float2, double>(D, TR, ssz, L);
         return group_smem_bytes<float2, float>(D, TR, ssz, L);
     };
-    int L = std::min(gp.L, GROUP_MAX_L);
+    int L = std::min(gp.L, std::min(lcap, GROUP_MAX_L));
     while (L > 6 && smem_at(L) > GROUP_SMEM_PREF) L--;
     if (smem_at(L) > GROUP_SMEM_BUDGET || L < 6) return false;
     GroupArgs &ga = op.ga;
@@ -480,6 +488,7 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
     op.k0 = gp.k0;
     op.d = gp.ws;
     op.tr = gp.d - gp.ws;
+    op.lcap = lcap;
     op.smem = smem_at(L);
     op.ntiles = 1u << ga.nbhi;
     if (E.prec == 128) op.fn = pick_group<double2, double>(op.d, op.tr);
@@ -494,6 +503,39 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
     return true;
 }
 
+static double single_entries(const HPlan &p, int k) {
+    const HStep &hs = p.st[(size_t)k];
+    const int r = hs.nk + (hs.tqs.size() == 4 ? 2 : hs.tqs.size() == 2 ? 1 : 0);
+    return std::ldexp(1.0, r) + std::ldexp(1.0, hs.nk + (hs.m == 2 ? 1 : 0));
+}
+
+// The pass of a shape with the engine's current matrices; false when the group cannot be built.
+static bool make_op(Engine &E, const OpShape &sh, Op &op) {
+    op = Op();
+    if (!sh.group) {
+        op.k0 = sh.k0;
+        op.d = 1;
+        op.entries = single_entries(E.plan, sh.k0);
+        return true;
+    }
+    GroupPlan gp;
+    if (!plan_group(E.plan, sh.k0, sh.d + sh.tr, 6, sh.lcap, gp, sh.d) || !fill_group(E, gp, op, sh.lcap)) return false;
+    op.norm_first = sh.norm_first;
+    op.ga.src = sh.src;
+    return true;
+}
+
+static bool ops_from_shapes(Engine &E, const std::vector<OpShape> &shapes, std::vector<Op> &ops) {
+    std::vector<Op> out;
+    for (const OpShape &sh : shapes) {
+        Op op;
+        if (!make_op(E, sh, op)) return false;
+        out.push_back(op);
+    }
+    ops.swap(out);
+    return true;
+}
+
 // Sampling pass list ('prob' / 'sample'): the cheapest cover of the steps, by table entries moved, with
 //   * single steps: norm pass + write pass (read, read, write);
 //   * fused passes of steps k .. k+d-1 (k+1 .. k+d-1 analytic, so their bits need no data), optionally with the
@@ -501,6 +543,7 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op) {
 //     the previous pass's trailing norms, from M when step k is analytic, or else from a norm pass launched first.
 static void build_sample_ops(Engine &E) {
     E.sample_ops.clear();
+    if (!E.sample_shapes.empty() && ops_from_shapes(E, E.sample_shapes, E.sample_ops)) return;
     if (E.fuse_depth < 2) return;
     const HPlan &p = E.plan;
     const int ns = p.ns;
@@ -556,6 +599,7 @@ static void build_sample_ops(Engine &E) {
 static void build_chain_ops(Engine &E) {
     build_sample_ops(E);
     E.chain_ops.clear();
+    if (!E.chain_shapes.empty() && ops_from_shapes(E, E.chain_shapes, E.chain_ops)) return;
     const HPlan &p = E.plan;
     for (int k = 0; k < p.ns;) {
         const HStep &hs = p.st[(size_t)k];
@@ -1091,10 +1135,247 @@ int gsb_set_fusion(gsb_engine *e, int depth) {
     DevGuard g(E->dev);
     GSB_CK(cudaStreamSynchronize(E->stream));
     E->fuse_depth = depth;
+    E->chain_shapes.clear();     // an explicit depth replaces the autotuner's choice
+    E->sample_shapes.clear();
     for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);
     E->graphs.clear();
     build_chain_ops(*E);
     return 0;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------
+// Autotuner of the pass lists: every candidate pass (one step; 2 or 3 fused steps; with or without the next step's
+// branch norms for sampling; tile caps 2^8, 2^9, 2^10) is timed on the device, alone, with CUDA events on the
+// engine's stream, and the cover of the steps with the least measured time replaces the byte-model choice.  A pass's
+// time does not depend on the table's values (no data-dependent control flow besides the dead flag, which the device
+// state reset before each launch clears), so the candidates run on whatever the arena holds, with bits chosen so that
+// no analytic step takes a zero-probability branch.
+
+struct Timer {
+    Engine &E;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int reps;
+    explicit Timer(Engine &e, int r) : E(e), reps(r) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+    }
+    ~Timer() {
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    // mean milliseconds of `launch` after a device-state reset, or a negative value on a CUDA error
+    template <typename F>
+    double operator()(F launch) {
+        double tot = 0;
+        for (int r = -1; r < reps; r++) {   // r = -1: untimed warm-up
+            k_set_item<<<1, 1, 0, E.stream>>>(E.st, 0);
+            if (E.launch_begin() != cudaSuccess) return -1;
+            if (cudaEventRecord(e0, E.stream) != cudaSuccess) return -1;
+            if (launch() != cudaSuccess) return -1;
+            if (cudaEventRecord(e1, E.stream) != cudaSuccess) return -1;
+            if (cudaEventSynchronize(e1) != cudaSuccess) return -1;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (r >= 0) tot += ms;
+        }
+        return tot / reps;
+    }
+};
+
+static int autotune(Engine &E, int mode, int reps) {
+    const HPlan &p = E.plan;
+    const int ns = p.ns;
+    if (ns < 1) return 0;
+    // forced bits for timing: the likelier branch of every analytic step, 0 elsewhere
+    std::vector<int8_t> row((size_t)ns, 0);
+    for (int k = 0; k < ns; k++) {
+        const HStep &h = p.st[(size_t)k];
+        const double c0 = h.Mr[0][0] * h.Mr[0][0] + h.Mi[0][0] * h.Mi[0][0] + h.Mr[0][1] * h.Mr[0][1] + h.Mi[0][1] * h.Mi[0][1];
+        const double c1 = h.Mr[1][0] * h.Mr[1][0] + h.Mi[1][0] * h.Mi[1][0] + h.Mr[1][1] * h.Mr[1][1] + h.Mi[1][1] * h.Mi[1][1];
+        row[(size_t)k] = (int8_t)(c1 > c0 ? 1 : 0);
+    }
+    GSB_CK(cudaMemcpyAsync(E.d_forced, row.data(), (size_t)ns, cudaMemcpyHostToDevice, E.stream));
+    Timer timer(E, reps);
+    auto rof = [&](int k) { const HStep &h = p.st[(size_t)k]; return h.nk + (h.tqs.size() == 4 ? 2 : h.tqs.size() == 2 ? 1 : 0); };
+    const double INF = 1e300;
+    std::vector<double> t_write((size_t)ns), t_norm((size_t)ns);
+    const int drv = mode == 0 ? DRV_CHAIN1 : DRV_CHAIN;
+    for (int k = 0; k < ns; k++) {
+        t_write[(size_t)k] = timer([&] { return E.launch_step(k, true, drv, ns, true, false); });
+        t_norm[(size_t)k] = mode == 0 ? 0 : timer([&] { return E.launch_step(k, false, drv, ns, true, false); });
+        if (t_write[(size_t)k] < 0 || t_norm[(size_t)k] < 0) return fail(GSB_E_CUDA, "autotuner: a timing launch failed");
+    }
+    // fused candidates starting at k, with their times (distinct tile sizes only)
+    auto fused = [&](int k, int d, int tr, std::vector<std::pair<OpShape, double>> &out) -> int {
+        int lastL = -1;
+        for (int lcap : {GROUP_MAX_L, GROUP_MAX_L - 1, GROUP_MAX_L - 2}) {
+            OpShape sh;
+            sh.group = true;
+            sh.k0 = k;
+            sh.d = d;
+            sh.tr = tr;
+            sh.lcap = lcap;
+            sh.src = GSRC_NORM;   // timing: the bit of step k as a norm pass would leave it
+            Op op;
+            if (!make_op(E, sh, op) || op.ga.L == lastL) continue;
+            lastL = op.ga.L;
+            const double t = timer([&] { return E.launch_op(op, drv, true, false); });
+            if (t < 0) return fail(GSB_E_CUDA, "autotuner: a timing launch failed");
+            out.push_back({sh, t});
+        }
+        return 0;
+    };
+    if (mode == 0) {
+        std::vector<double> cost((size_t)ns + 1, INF);
+        std::vector<OpShape> pick((size_t)ns + 1);
+        cost[(size_t)ns] = 0;
+        for (int k = ns - 1; k >= 0; k--) {
+            OpShape single;
+            single.k0 = k;
+            cost[(size_t)k] = t_write[(size_t)k] + cost[(size_t)k + 1];
+            pick[(size_t)k] = single;
+            if (rof(k) < GROUP_MIN_R) continue;
+            for (int d = 2; d <= FUSE_MAX_STEPS && k + d <= ns; d++) {
+                std::vector<std::pair<OpShape, double>> c;
+                if (int rc = fused(k, d, 0, c)) return rc;
+                for (auto &x : c)
+                    if (x.second + cost[(size_t)(k + d)] < cost[(size_t)k]) {
+                        cost[(size_t)k] = x.second + cost[(size_t)(k + d)];
+                        pick[(size_t)k] = x.first;
+                    }
+            }
+        }
+        E.chain_shapes.clear();
+        for (int k = 0; k < ns;) {
+            E.chain_shapes.push_back(pick[(size_t)k]);
+            k += pick[(size_t)k].group ? pick[(size_t)k].d : 1;
+        }
+        return 0;
+    }
+    // sampling: state t = step k's branch norms come from the previous pass
+    std::vector<std::array<double, 2>> cost((size_t)ns + 1, {INF, INF});
+    std::vector<std::array<OpShape, 2>> pick((size_t)ns + 1);
+    cost[(size_t)ns] = {0, 0};
+    std::vector<std::vector<std::pair<OpShape, double>>> cands((size_t)ns);
+    for (int k = 0; k < ns; k++) {
+        if (rof(k) < GROUP_MIN_R) continue;
+        for (int d = 1; d <= FUSE_MAX_STEPS && k + d <= ns; d++) {
+            if (d > 1 && !analytic_step(p.st[(size_t)(k + d - 1)])) break;
+            for (int tr = 0; tr < 2; tr++) {
+                if (d + tr < 2 || d + tr > FUSE_MAX_STEPS) continue;
+                if (tr && (k + d >= ns || analytic_step(p.st[(size_t)(k + d)]))) continue;
+                if (int rc = fused(k, d, tr, cands[(size_t)k])) return rc;
+            }
+        }
+    }
+    for (int k = ns - 1; k >= 0; k--) {
+        const bool an = analytic_step(p.st[(size_t)k]);
+        for (int t = 0; t < 2; t++) {
+            OpShape single;
+            single.k0 = k;
+            double best = t_norm[(size_t)k] + t_write[(size_t)k] + cost[(size_t)k + 1][0];
+            OpShape bp = single;
+            for (auto &x : cands[(size_t)k]) {
+                const OpShape &sh = x.first;
+                const bool nf = !an && !t;
+                const double c = (nf ? t_norm[(size_t)k] : 0) + x.second + cost[(size_t)(k + sh.d)][(size_t)sh.tr];
+                if (c < best) {
+                    best = c;
+                    bp = sh;
+                    bp.norm_first = nf;
+                    bp.src = an ? GSRC_ANALYTIC : t ? GSRC_TRAILING : GSRC_NORM;
+                }
+            }
+            cost[(size_t)k][(size_t)t] = best;
+            pick[(size_t)k][(size_t)t] = bp;
+        }
+    }
+    E.sample_shapes.clear();
+    for (int k = 0, t = 0; k < ns;) {
+        const OpShape &sh = pick[(size_t)k][(size_t)t];
+        E.sample_shapes.push_back(sh);
+        t = sh.group ? sh.tr : 0;
+        k += sh.group ? sh.d : 1;
+    }
+    return 0;
+}
+
+extern "C" {
+
+int gsb_autotune(gsb_engine *e, int mode, int reps, float *ms_before, float *ms_after) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    if (mode < 0 || mode > 2 || reps < 1) return fail(GSB_E_USAGE, "mode must be 0 (chain), 1 (sampling) or 2 (both)");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    const HPlan &p = E->plan;
+    {   // the timed items' bits: the likelier branch of every analytic step, 0 elsewhere (as the autotuner uses)
+        std::vector<int8_t> row((size_t)std::max(p.ns, 1), 0);
+        for (int k = 0; k < p.ns; k++) {
+            const HStep &h = p.st[(size_t)k];
+            const double c0 = h.Mr[0][0] * h.Mr[0][0] + h.Mi[0][0] * h.Mi[0][0] + h.Mr[0][1] * h.Mr[0][1] + h.Mi[0][1] * h.Mi[0][1];
+            const double c1 = h.Mr[1][0] * h.Mr[1][0] + h.Mi[1][0] * h.Mi[1][0] + h.Mr[1][1] * h.Mr[1][1] + h.Mi[1][1] * h.Mi[1][1];
+            row[(size_t)k] = (int8_t)(c1 > c0 ? 1 : 0);
+        }
+        if (p.ns) GSB_CK(cudaMemcpyAsync(E->d_forced, row.data(), (size_t)p.ns, cudaMemcpyHostToDevice, E->stream));
+    }
+    // device time of one item of graph `kind` (replayed: one warm-up, then the mean of `reps`)
+    auto item_ms = [&](int kind, float *out) -> int {
+        cudaGraphExec_t ex;
+        if (int rc = E->graph(kind, &ex)) return rc;
+        cudaEvent_t a, b;
+        GSB_CK(cudaEventCreate(&a));
+        GSB_CK(cudaEventCreate(&b));
+        k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
+        GSB_CK(cudaGraphLaunch(ex, E->stream));
+        float tot = 0;
+        for (int r = 0; r < reps; r++) {
+            k_set_item<<<1, 1, 0, E->stream>>>(E->st, 0);
+            GSB_CK(cudaEventRecord(a, E->stream));
+            GSB_CK(cudaGraphLaunch(ex, E->stream));
+            GSB_CK(cudaEventRecord(b, E->stream));
+            GSB_CK(cudaEventSynchronize(b));
+            float ms = 0;
+            cudaEventElapsedTime(&ms, a, b);
+            tot += ms;
+        }
+        *out = tot / reps;
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        return 0;
+    };
+    auto rebuild = [&]() {
+        for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);
+        E->graphs.clear();
+        build_chain_ops(*E);
+    };
+    float tb = 0, ta = 0;
+    // per pass list: tune, then keep the tuned list only if a whole item got faster (passes timed alone do not
+    // always add up to their time in sequence)
+    for (int m = 0; m < 2; m++) {
+        if (mode != 2 && mode != m) continue;
+        const int kind = m == 0 ? 0 : 1;   // the 'chain' graph, or 'prob' (the sampling passes with forced bits)
+        float before = 0, after = 0;
+        if (int rc = item_ms(kind, &before)) return rc;
+        std::vector<OpShape> keep = m == 0 ? E->chain_shapes : E->sample_shapes;
+        rebuild();
+        if (int rc = autotune(*E, m, reps)) return rc;
+        rebuild();
+        if (int rc = item_ms(kind, &after)) return rc;
+        if (after > before) {
+            (m == 0 ? E->chain_shapes : E->sample_shapes) = keep;
+            rebuild();
+            after = before;
+        }
+        tb += before;
+        ta += after;
+    }
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    if (ms_before) *ms_before = tb;
+    if (ms_after) *ms_after = ta;
+    return check_device(E);
 }
 
 int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries) {

@@ -74,6 +74,7 @@ def _load():
         "gsb_grad_close": (c.c_int, [P]),
         "gsb_grad_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_grad_run": (c.c_int, [P, dp, c.POINTER(c.c_int8), c.c_int64, dp, dp]),
+        "gsb_autotune": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_batch_open": (c.c_int, [c.POINTER(c.c_char_p), c.POINTER(c.c_size_t), c.c_int, c.c_int, c.c_int,
                                      c.POINTER(P)]),
         "gsb_batch_close": (c.c_int, [P]),
@@ -103,7 +104,7 @@ EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "g
            "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
-           "gsb_grad_run", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
+           "gsb_grad_run", "gsb_autotune", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
            "gsb_batch_set_shape", "gsb_batch_get_shape", "gsb_batch_tune")
 
 
@@ -306,6 +307,13 @@ class Engine:
     def set_fusion(self, depth):
         """'chain' mode: fuse up to `depth` consecutive wide steps per pass (1 = no fusion)."""
         _check(_lib.gsb_set_fusion(self.handle, int(depth)))
+
+    def autotune(self, mode=2, reps=3):
+        """Time every candidate pass on this device and keep the fastest covers of the steps (mode 0: 'chain',
+        1: 'prob' / 'sample', 2: both); returns (ms of one item before, after)."""
+        a, b = ctypes.c_float(), ctypes.c_float()
+        _check(_lib.gsb_autotune(self.handle, int(mode), int(reps), ctypes.byref(a), ctypes.byref(b)))
+        return a.value, b.value
 
     def fusion_groups(self):
         """(group length per step: the pass starting at step k spans that many steps, 0 inside a pass;

@@ -116,6 +116,14 @@ int gsb_set_stream(gsb_engine *e, void *cuda_stream);
  * the arena: the intermediate tables of a group live in shared-memory tiles only.  depth 1 disables fusion;
  * default 2.  Results are those of the unfused steps up to rounding. */
 int gsb_set_fusion(gsb_engine *e, int depth);
+/* Autotune the pass lists on this device: every candidate pass (one step; 2 or 3 fused steps; for sampling with or
+ * without the next step's branch norms; tiles of up to 2^8, 2^9 or 2^10 classes) is timed alone with CUDA events,
+ * and the covers of the steps with the least measured time replace the byte-model choice (mode 0: 'chain' passes,
+ * 1: 'prob' / 'sample' passes, 2: both) -- if a whole item, replayed, gets faster; otherwise the previous list
+ * stays.  The choice survives gsb_set_matrices; gsb_set_fusion discards it.  ms_before / ms_after (may be NULL):
+ * device time of one item of each tuned list before and after (summed for mode 2).  No counterpart in the
+ * reference. */
+int gsb_autotune(gsb_engine *e, int mode, int reps, float *ms_before, float *ms_after);
 /* Pass structure of 'chain' mode: group_len[k] = number of steps of the pass starting at step k (0 inside a pass);
  * entries[k] (may be NULL) = table entries the pass reads plus writes. */
 int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries);

@@ -152,7 +152,7 @@ def test_statevector_n24():
 def test_fused_chain_depths_vs_oracle(wide_case, mode):
     """'chain' mode with 1, 2 and 3 DP steps fused per pass gives the oracle's log2 Pr and conditionals; 'prob' and
     'sample' (fused passes that carry the next step's branch norms) give the oracle's probabilities and
-    bit-identical samples."""
+    bit-identical samples; so do the pass lists the autotuner picks."""
     import workloads
     from oracle import Oracle
     ns = n = len(wide_case["steps"])
@@ -179,3 +179,20 @@ def test_fused_chain_depths_vs_oracle(wide_case, mode):
             for i in range(4):
                 ob, olp = samples_ref[i]
                 assert list(bits[i]) == list(ob) and abs(slp[i] - olp) <= lp_tol(mode, olp, n), (depth, i)
+        # the autotuner's pass lists (measured on this device) must give the same results
+        before, after = eng.autotune(mode=2, reps=1)
+        assert before > 0 and after > 0
+        glen, _ = eng.fusion_groups()
+        assert sum(glen) == ns
+        lp, cond = eng.chain(strings)
+        for i, (olp, ocond) in enumerate(ref):
+            assert abs(lp[i] - olp) <= lp_tol(mode, olp, n), ("tuned", i, lp[i], olp)
+            if olp > -n - 3:
+                assert np.abs(cond[i] - ocond).max() <= cond_tol(mode)
+        lpp = eng.prob(strings[:4])
+        for i in range(4):
+            assert abs(lpp[i] - ref[i][0]) <= lp_tol(mode, ref[i][0], n), ("tuned", i)
+        bits, slp = eng.sample(4, 123)
+        for i in range(4):
+            ob, olp = samples_ref[i]
+            assert list(bits[i]) == list(ob) and abs(slp[i] - olp) <= lp_tol(mode, olp, n), ("tuned", i)
