@@ -46,7 +46,7 @@ import replicas  # noqa: E402  (package module: torchrun rank bookkeeping)
 
 METRIC = "s/sample & amps/s at n=70 w=30, c64 form vs c128 plain, |Δlog2P|≤1e-5; HBM GB/s"
 WORKLOAD = "matching_n70_d70_s2_w30"
-K_GROUP_TRAFFIC_RATIO = 0.9734
+K_GROUP_TRAFFIC_RATIO = 0.9722
 
 
 def parse():
@@ -300,7 +300,7 @@ def run_gsb(args):
     fused_bytes = float(sum(gent[k] for k in fused)) * 8
     fused_ms = float(sum(wmean[k] for k in fused))
     # DRAM bytes per algorithmic byte of the dominant pass, from one ncu capture of k_group<float2, float, 2, 0> on the
-    # width-27 instance (2.0903 GB read + written for 2.1475 GB algorithmic: no re-reads; writes still dirty in L2
+    # width-27 instance (2.0880 GB read + written for 2.1475 GB algorithmic: no re-reads; writes still dirty in L2
     # at kernel end make it < 1), scaled to the chain passes of one string
     traffic = pass_bytes * K_GROUP_TRAFFIC_RATIO
     # exact-sample passes (a norm pass where a pass has no other source for its first bit, then the pass)
