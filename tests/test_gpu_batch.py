@@ -62,3 +62,21 @@ def test_batch_shapes_and_c64(small_batch):
     # complex64 (FP32 sums, FP64 norms and scales) against complex128; log2 amplifies the rounding of unlikely
     # strings, so the bound scales with -log2 Pr
     assert np.all(d <= 2e-5 * np.maximum(1.0, -want / 10)), float(d.max())
+
+
+def test_batch_single_prefix_single_suffix_and_longest_prefix():
+    """npre = nsuf = 1 and K = ns - 1 (a one-step suffix) against the single-plan executor (complex128)."""
+    import gsb
+    import workloads
+    bw = workloads.batch_workload(count=5, seed=11, nmin=16, nmax=24, npre=1, nsuf=1, iters=2000)
+    K = [len(w["steps"]) - 1 for w in bw["instances"]]
+    rng = np.random.default_rng(2)
+    pre = [rng.integers(0, 2, size=(1, k), dtype=np.int8) for k in K]
+    suf = [rng.integers(0, 2, size=(1, 1, 1), dtype=np.int8) for _ in K]
+    b = gsb.Batch([w["plan"] for w in bw["instances"]], precision=gsb.GSB_C128)
+    b.set_strings(K, pre, suf)
+    lp, _ = b.run()
+    for i, w in enumerate(bw["instances"]):
+        with gsb.Engine.from_text(w["plan"], precision=gsb.GSB_C128) as eng:
+            want = eng.chain(np.concatenate([pre[i][0], suf[i][0, 0]])[None, :])[0][0]
+        assert abs(lp[i, 0, 0] - want) <= 1e-9 or (not np.isfinite(want) and not np.isfinite(lp[i, 0, 0]))

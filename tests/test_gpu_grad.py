@@ -95,3 +95,20 @@ def test_gradient_matches_finite_differences_n48():
         fd = (float(_loss(tp, w, bits, sweep)) - float(_loss(tm, w, bits, sweep))) / (2 * h)
         # central differences: error O(h^2) times the third derivative
         assert abs(fd - float(th.grad[q, a])) < 1e-4 * max(1.0, abs(fd)), (q, a, fd, float(th.grad[q, a]))
+
+
+def test_checkpoint_interval_and_partial_batches_do_not_change_gradients():
+    """every = 1 (a checkpoint before every step), 3 and 64 (one segment: the whole sweep recomputed once) give the
+    same Z and dZ; 37 strings (not a multiple of the strings swept per launch) give the same rows as 5 of them."""
+    import adjoint
+    import gsb
+    w = _instance(20, 5)
+    bits = _targets(w, 37, 4)
+    M = adjoint.step_matrices(torch.tensor(w["theta0"]), w["M0"], w["step_vertices"]).numpy()
+    ref_z, ref_dz = gsb.GradSweep(w["plan"], every=4).run(M, bits)
+    for every in (1, 3, 64):
+        z, dz = gsb.GradSweep(w["plan"], every=every).run(M, bits)
+        assert np.max(np.abs(z - ref_z)) <= 1e-12 * np.max(np.abs(ref_z))
+        assert np.max(np.abs(dz - ref_dz)) <= 1e-12 * np.max(np.abs(ref_dz))
+    z5, dz5 = gsb.GradSweep(w["plan"], every=4).run(M, bits[:5])
+    assert np.array_equal(z5, ref_z[:5]) and np.array_equal(dz5, ref_dz[:5])

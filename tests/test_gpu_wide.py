@@ -196,3 +196,8 @@ def test_fused_chain_depths_vs_oracle(wide_case, mode):
         for i in range(4):
             ob, olp = samples_ref[i]
             assert list(bits[i]) == list(ob) and abs(slp[i] - olp) <= lp_tol(mode, olp, n), ("tuned", i)
+        # new matrices keep the tuned pass lists (rebuilt with the new M): the same plan's M gives the same results
+        tuned = eng.fusion_groups()[0]
+        eng.set_matrices_from_text(open(wide_case["path"]).read())
+        assert eng.fusion_groups()[0] == tuned
+        assert np.array_equal(eng.chain(strings)[0], lp)
