@@ -306,6 +306,8 @@ def run_gsb(args):
     # exact-sample passes (a norm pass where a pass has no other source for its first bit, then the pass)
     sw, sn = eng.profile_steps(strings[0], mode=1)
     sample_kernel_ms = float(sw.sum() + sn.sum())
+    _, sent = eng.sample_groups()
+    sample_pass_bytes = float(np.sum(sent)) * 8
     sample_bytes = float(sum((2 * (1 << st["r"]) + (1 << st["rn"])) for st in steps)) * 8
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm_peak, "unit": "GB/s", "frac": achieved / hbm_peak,
                 "traffic": traffic, "traffic_source": "ncu dram bytes of one k_group launch (width-27 capture) per "
@@ -318,7 +320,10 @@ def run_gsb(args):
                 "unfused_model_GBps": float(sum(p[0] for p in per)) / (kernel_ms / 1000.0) / 1e9,
                 "passes_per_string": int(sum(1 for x in glen if x > 0)), "fusion": args.fusion,
                 "sample_kernel_ms": sample_kernel_ms, "sample_norm_ms": float(sn.sum()),
-                "sample_write_ms": float(sw.sum()), "sample_unfused_model_bytes": sample_bytes}
+                "sample_write_ms": float(sw.sum()), "sample_unfused_model_bytes": sample_bytes,
+                "sample_pass_bytes": sample_pass_bytes,
+                "sample_achieved": sample_pass_bytes / (sample_kernel_ms / 1000.0) / 1e9,
+                "sample_frac": sample_pass_bytes / (sample_kernel_ms / 1000.0) / 1e9 / hbm_peak}
     eng.close()
 
     # complex128 plain form on the first strings of the timed batch, and the c64-vs-c128 agreement

@@ -1378,6 +1378,30 @@ int gsb_autotune(gsb_engine *e, int mode, int reps, float *ms_before, float *ms_
     return check_device(E);
 }
 
+int gsb_sample_groups(const gsb_engine *e, int *group_len, double *entries) {
+    if (!e || !group_len) return fail(GSB_E_USAGE, "null argument");
+    const Engine *E = eng(e);
+    const HPlan &p = E->plan;
+    for (int k = 0; k < p.ns; k++) {
+        group_len[k] = 0;
+        if (entries) entries[k] = 0;
+    }
+    auto table = [&](int k) { const HStep &h = p.st[(size_t)k]; return std::ldexp(1.0, h.nk) * (double)h.tqs.size(); };
+    if (E->sample_ops.empty()) {   // no fusion: a norm pass and a write pass per step
+        for (int k = 0; k < p.ns; k++) {
+            group_len[k] = 1;
+            if (entries) entries[k] = table(k) + single_entries(p, k);
+        }
+        return 0;
+    }
+    for (const Op &op : E->sample_ops) {
+        group_len[op.k0] = op.group ? op.d : 1;
+        if (entries) entries[op.k0] = (op.group ? op.entries : single_entries(p, op.k0)) +
+                                      ((!op.group || op.norm_first) ? table(op.k0) : 0.0);
+    }
+    return 0;
+}
+
 int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries) {
     if (!e || !group_len) return fail(GSB_E_USAGE, "null argument");
     const Engine *E = eng(e);

@@ -127,6 +127,9 @@ int gsb_autotune(gsb_engine *e, int mode, int reps, float *ms_before, float *ms_
 /* Pass structure of 'chain' mode: group_len[k] = number of steps of the pass starting at step k (0 inside a pass);
  * entries[k] (may be NULL) = table entries the pass reads plus writes. */
 int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries);
+/* The same for the sampling passes ('prob' / 'sample'): group_len[k] = steps written by the pass starting at step k;
+ * entries[k] = table entries it reads plus writes, including the norm pass launched before it where it has one. */
+int gsb_sample_groups(const gsb_engine *e, int *group_len, double *entries);
 /* Replace every step's rotation matrix: M is [nsteps][2][2] complex (re, im), M[k][b][x] as the plan text lists
  * it.  The layout stays; this is how one engine (one arena) serves all slice plans of make_sliced_plans, which
  * share the layout and differ only in M (sliced_plans.py:1-14). */
