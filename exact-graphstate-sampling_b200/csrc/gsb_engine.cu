@@ -153,6 +153,7 @@ struct Engine {
     int fuse_depth = 2;                  // chain mode: largest number of DP steps fused into one pass (1 = none)
     std::vector<Op> chain_ops;           // 'chain' passes
     std::vector<Op> sample_ops;          // 'prob' / 'sample' passes (build_sample_ops)
+    int withhold_loads = 0;              // test hook: fused passes issue no tile loads (their bounded waits run out)
     std::vector<OpShape> chain_shapes;   // pass lists chosen by gsb_autotune (empty: the byte-model defaults)
     std::vector<OpShape> sample_shapes;
     size_t esize = 8;
@@ -273,6 +274,7 @@ struct Engine {
         L.nchunks = op.ntiles;
         Ctx c = ctx(driver, plan.ns, L, use_forced, use_unif);
         GroupArgs ga = op.ga;
+        ga.withhold_loads = withhold_loads;
         void *memp = mem;
         void *kargs[] = {&ga, &memp, &c};
         return cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, stream);
@@ -1376,6 +1378,17 @@ int gsb_autotune(gsb_engine *e, int mode, int reps, float *ms_before, float *ms_
     if (ms_before) *ms_before = tb;
     if (ms_after) *ms_after = ta;
     return check_device(E);
+}
+
+int gsb_test_withhold_tile_loads(gsb_engine *e, int on) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    E->withhold_loads = on ? 1 : 0;
+    for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);   // the graphs hold the pass arguments by value
+    E->graphs.clear();
+    return 0;
 }
 
 int gsb_sample_groups(const gsb_engine *e, int *group_len, double *entries) {

@@ -31,6 +31,7 @@ enum { GSRC_ANALYTIC = 0, GSRC_TRAILING = 1, GSRC_NORM = 2 };
 struct GroupArgs {
     int d, L, nbhi, ssz[4];
     int src;               // GSRC_*
+    int withhold_loads;    // test hook (gsb_test_withhold_tile_loads): issue no tile loads, so every wait runs out
     uint64_t bhi[40];
     uint64_t blk_in[32];   // stage-0 offsets z_i, bits >= L: input block i of a tile is the arena block at TB ^ blk_in[i]
     uint64_t blk_out[32];  // written-stage offsets, bits >= L: output block i goes to the arena block at TB ^ blk_out[i]
@@ -585,7 +586,7 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
         for (int i = 0; i < ga.ssz[0]; i++) bulk_load(dst + (uint32_t)i * blk_bytes, mem + (TBn ^ ga.blk_in[i]), blk_bytes, bar);
     };
     int issued = 0;   // tiles whose loads thread 0 issued
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0 && !ga.withhold_loads)
         for (unsigned int n = i0; n < i1 && n < i0 + 2; n++) {
             issue_loads(n);
             issued++;
@@ -617,7 +618,7 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             group_cosets_any<E, T, true, false, true, 1, 1>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         }
-        if (threadIdx.x == 0 && it + 2 < i1) {
+        if (threadIdx.x == 0 && it + 2 < i1 && !ga.withhold_loads) {
             issue_loads(it + 2);
             issued++;
         }

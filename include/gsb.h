@@ -206,6 +206,12 @@ int gsb_batch_get_shape(const gsb_batch *b, int *block, int *small_R, int *per_s
  * keeps the fastest; returns it and its mean time. */
 int gsb_batch_tune(gsb_batch *b, int reps, size_t max_bytes, int *block, int *small_R, int *per_sm, float *best_ms);
 
+/* Test hook for the fused passes' failure path (no counterpart in the reference): with on != 0 the passes issue no
+ * tile loads, so every CTA's bounded wait runs out (about one second); the kernel records the failure, marks the
+ * item dead and returns, and the call reports GSB_E_CUDA.  Nothing faults or hangs and the engine stays usable; with
+ * on = 0 the passes run normally again. */
+int gsb_test_withhold_tile_loads(gsb_engine *e, int on);
+
 /* ---- host-side helpers (no GPU needed) ---- */
 
 /* Parse and validate a plan without allocating anything on a device: the same checks gsb_open_* makes
