@@ -419,7 +419,10 @@ def run_form_batch(args):
     widths = [w["width"] for w in bw["instances"]]
     b = gsb.Batch(plans, precision=gsb.GSB_C64)
     b.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
-    block, small_R, per_sm, tune_ms = b.tune(reps=2)
+    if args.autotune:
+        block, small_R, per_sm, tune_ms = b.tune(reps=2)
+    else:
+        block, small_R, per_sm = b.shape()
     for _ in range(max(3, args.warmup)):
         b.run()
     times = []

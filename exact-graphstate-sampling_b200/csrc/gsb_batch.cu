@@ -63,6 +63,7 @@ struct BatchArgs {
 struct BlockTeam {
     __device__ int rank() const { return threadIdx.x; }
     __device__ int size() const { return blockDim.x; }
+    __device__ int log2size() const { return __ffs((int)blockDim.x) - 1; }   // blockDim.x: a power of two
     __device__ void sync() const { __syncthreads(); }
     __device__ double sum(double v) const {
         __shared__ double red[32];
@@ -80,6 +81,7 @@ struct BlockTeam {
 struct WarpTeam {
     __device__ int rank() const { return threadIdx.x & 31; }
     __device__ int size() const { return 32; }
+    __device__ int log2size() const { return 5; }
     __device__ void sync() const { __syncwarp(); }
     __device__ double sum(double v) const {
         __syncwarp();
@@ -107,36 +109,53 @@ __device__ __forceinline__ uint64_t bcoset_base(const uint64_t *tk, uint64_t c) 
     return b;
 }
 
+// The cosets of a step a team member visits: c = rank | (g << log2 team size) for the Gray codes g of the high bits,
+// so consecutive cosets differ in one high bit and the base is the member's fixed low part XOR one running value
+// (one XOR per coset instead of a loop over the bits of c).  f(c, base) is called for each.
+template <typename TM, typename F>
+__device__ __forceinline__ void team_cosets(const TM &tm, int nk, const uint64_t *tk, F f) {
+    const int ls = tm.log2size();
+    const uint64_t r = (uint64_t)tm.rank();
+    if (nk < ls && r >= (1ULL << nk)) return;
+    const uint64_t lo = bcoset_base(tk, r);
+    const uint64_t nh = nk > ls ? 1ULL << (nk - ls) : 1;
+    uint64_t hi = 0;
+    for (uint64_t n = 0; n < nh; n++) {
+        if (n) hi ^= tk[ls + __ffsll((long long)n) - 1];
+        f(r | ((n ^ (n >> 1)) << ls), lo ^ hi);
+    }
+}
+
 // One write pass of step s with bit `bit`, outputs scaled by `scale`; returns the written norm (to every thread).
 template <typename E, typename TM>
 __device__ double team_step(const TM &tm, const BStep &s, const uint64_t *tk, E *arena, int bit, double scale) {
     typedef typename ArithOf<E>::T T;
     const T m0r = (T)(scale * s.M[4 * bit + 0]), m0i = (T)(scale * s.M[4 * bit + 1]);
     const T m1r = (T)(scale * s.M[4 * bit + 2]), m1i = (T)(scale * s.M[4 * bit + 3]);
-    const uint64_t N = 1ULL << s.nk;
     double nb = 0;
-    for (uint64_t c = (uint64_t)tm.rank(); c < N; c += (uint64_t)tm.size()) {
-        const uint64_t base = bcoset_base(tk, c);
+    team_cosets(tm, s.nk, tk, [&](uint64_t c, uint64_t base) {
         const int pc = __popcll(c & s.rhoc) & 1;
-        T x0r[2] = {0, 0}, x0i[2] = {0, 0}, x1r[2] = {0, 0}, x1i[2] = {0, 0};
+        // x = 0 and signed x = 1 sums of the two outputs, in scalars (no runtime-indexed arrays)
+        T a0r = 0, a0i = 0, a1r = 0, a1i = 0, b0r = 0, b0i = 0, b1r = 0, b1i = 0;
         for (int t = 0; t < s.ntq; t++) {
             T vr, vi;
             ld_e(arena, base ^ s.tq[t], vr, vi);
-            x0r[s.tau0[t]] += vr;
-            x0i[s.tau0[t]] += vi;
-            const T sg = (pc ^ s.par[t]) ? (T)-1 : (T)1;
-            x1r[s.tau1[t]] += sg * vr;
-            x1i[s.tau1[t]] += sg * vi;
+            if (s.tau0[t]) { a1r += vr; a1i += vi; } else { a0r += vr; a0i += vi; }
+            if ((pc ^ s.par[t]) & 1) { vr = -vr; vi = -vi; }
+            if (s.tau1[t]) { b1r += vr; b1i += vi; } else { b0r += vr; b0i += vi; }
         }
-        T n = 0;
-        for (int tau = 0; tau < s.m; tau++) {
-            const T r = m0r * x0r[tau] - m0i * x0i[tau] + m1r * x1r[tau] - m1i * x1i[tau];
-            const T i = m0r * x0i[tau] + m0i * x0r[tau] + m1r * x1i[tau] + m1i * x1r[tau];
-            st_e(arena, tau ? base ^ s.g : base, r, i);
-            n += r * r + i * i;
+        const T r0 = m0r * a0r - m0i * a0i + m1r * b0r - m1i * b0i;
+        const T i0 = m0r * a0i + m0i * a0r + m1r * b0i + m1i * b0r;
+        st_e(arena, base, r0, i0);
+        T n = r0 * r0 + i0 * i0;
+        if (s.m == 2) {
+            const T r1 = m0r * a1r - m0i * a1i + m1r * b1r - m1i * b1i;
+            const T i1 = m0r * a1i + m0i * a1r + m1r * b1i + m1i * b1r;
+            st_e(arena, base ^ s.g, r1, i1);
+            n += r1 * r1 + i1 * i1;
         }
         nb += (double)n;
-    }
+    });
     tm.sync();
     return tm.sum(nb);
 }
@@ -144,14 +163,12 @@ __device__ double team_step(const TM &tm, const BStep &s, const uint64_t *tk, E 
 // Live table before step s, in (coset, offset) order, to / from a compact buffer.
 template <typename E, typename TM>
 __device__ void team_copy(const TM &tm, const BStep &s, const uint64_t *tk, E *arena, E *snap, bool save) {
-    const uint64_t N = 1ULL << s.nk;
-    for (uint64_t c = (uint64_t)tm.rank(); c < N; c += (uint64_t)tm.size()) {
-        const uint64_t base = bcoset_base(tk, c);
+    team_cosets(tm, s.nk, tk, [&](uint64_t c, uint64_t base) {
         for (int t = 0; t < s.ntq; t++) {
             if (save) snap[c * (uint64_t)s.ntq + (uint64_t)t] = arena[base ^ s.tq[t]];
             else arena[base ^ s.tq[t]] = snap[c * (uint64_t)s.ntq + (uint64_t)t];
         }
-    }
+    });
     tm.sync();
 }
 
