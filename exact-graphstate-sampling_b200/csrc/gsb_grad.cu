@@ -50,6 +50,23 @@ __device__ __forceinline__ uint64_t coset_base(const StepArgs &s, uint64_t c) {
     return b;
 }
 
+// The cosets a thread visits (grid x times block: a power of two, 2^ls threads): c = t | (g << ls) for the Gray
+// codes g of the high bits, so the base is the thread's fixed low part XOR one running value (one XOR per coset).
+template <typename F>
+__device__ __forceinline__ void grid_cosets(const StepArgs &s, F f) {
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const int ls = __ffsll((long long)nthreads) - 1;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s.nk < ls && t >= (1ULL << s.nk)) return;
+    const uint64_t lo = coset_base(s, t);
+    const uint64_t nh = s.nk > ls ? 1ULL << (s.nk - ls) : 1;
+    uint64_t hi = 0;
+    for (uint64_t n = 0; n < nh; n++) {
+        if (n) hi ^= s.tk[ls + __ffsll((long long)n) - 1];
+        f(t | ((n ^ (n >> 1)) << ls), lo ^ hi);
+    }
+}
+
 __device__ __forceinline__ void step_row(const StepArgs &s, const GradCtx &g, double2 &m0, double2 &m1) {
     const int b = g.bits[(size_t)(*g.item + (int)blockIdx.y) * (size_t)g.ns + (size_t)s.k];
     const double *Mk = g.M + (size_t)s.k * 8 + 4 * b;
@@ -73,23 +90,20 @@ __global__ void __launch_bounds__(256) k_gr_fwd(const StepArgs s, double2 *__res
     step_row(s, g, m0, m1);
     T += blockIdx.y * g.arena;
     if (gather) gather += blockIdx.y * gather_stride;
-    const uint64_t N = 1ULL << s.nk;
-    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t base = coset_base(s, c);
+    grid_cosets(s, [&](uint64_t c, uint64_t base) {
         const int pc = __popcll(c & s.rhoc) & 1;
-        double2 v[4];
-        for (int t = 0; t < s.ntq; t++) v[t] = T[base ^ s.tq[t]];
-        if (gather)
-            for (int t = 0; t < s.ntq; t++) gather[c * (uint64_t)s.ntq + (uint64_t)t] = v[t];
-        if (!write) continue;
-        double2 o[2] = {make_double2(0, 0), make_double2(0, 0)};
+        double2 o0 = make_double2(0, 0), o1 = make_double2(0, 0);   // scalars: no runtime-indexed arrays
         for (int t = 0; t < s.ntq; t++) {
-            o[s.tau0[t]] = cadd(o[s.tau0[t]], cmul(m0, v[t]));
-            o[s.tau1[t]] = cadd(o[s.tau1[t]], cscale((pc ^ s.par[t]) ? -1.0 : 1.0, cmul(m1, v[t])));
+            const double2 v = T[base ^ s.tq[t]];
+            if (gather) gather[c * (uint64_t)s.ntq + (uint64_t)t] = v;
+            const double2 a = cmul(m0, v), b = cscale((pc ^ s.par[t]) ? -1.0 : 1.0, cmul(m1, v));
+            if (s.tau0[t]) o1 = cadd(o1, a); else o0 = cadd(o0, a);
+            if (s.tau1[t]) o1 = cadd(o1, b); else o0 = cadd(o0, b);
         }
-        T[base] = o[0];
-        if (s.m == 2) T[base ^ s.g] = o[1];
-    }
+        if (!write) return;
+        T[base] = o0;
+        if (s.m == 2) T[base ^ s.g] = o1;
+    });
 }
 
 // Restore a checkpoint: the compact table [c][t] back to its arena slots.
@@ -97,11 +111,9 @@ __global__ void __launch_bounds__(256) k_gr_scatter(const StepArgs s, const doub
                                                     double2 *__restrict__ T, const GradCtx g) {
     src += blockIdx.y * src_stride;
     T += blockIdx.y * g.arena;
-    const uint64_t N = 1ULL << s.nk;
-    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t base = coset_base(s, c);
+    grid_cosets(s, [&](uint64_t c, uint64_t base) {
         for (int t = 0; t < s.ntq; t++) T[base ^ s.tq[t]] = src[c * (uint64_t)s.ntq + (uint64_t)t];
-    }
+    });
 }
 
 // End of the forward sweep: Z = T[0]; lambda_ns = 1.
@@ -125,26 +137,22 @@ __global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 
     Lam += blockIdx.y * g.arena;
     partials += (size_t)blockIdx.y * 4 * (size_t)g.maxgrid;
     counter += blockIdx.y;
-    const uint64_t N = 1ULL << s.nk;
     double a[4] = {0, 0, 0, 0};   // dZ/dm0 (re, im), dZ/dm1 (re, im)
-    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < N; c += (uint64_t)gridDim.x * blockDim.x) {
-        const uint64_t base = coset_base(s, c);
+    grid_cosets(s, [&](uint64_t c, uint64_t base) {
         const int pc = __popcll(c & s.rhoc) & 1;
-        const double2 lam[2] = {Lam[base], s.m == 2 ? Lam[base ^ s.g] : make_double2(0, 0)};
-        double2 nl[4];
+        const double2 lam0 = Lam[base], lam1 = s.m == 2 ? Lam[base ^ s.g] : make_double2(0, 0);   // read first
         for (int t = 0; t < s.ntq; t++) {
             const double2 v = Tk[c * (uint64_t)s.ntq + (uint64_t)t];
             const double sg = (pc ^ s.par[t]) ? -1.0 : 1.0;
-            const double2 la = lam[s.tau0[t]], lb = cscale(sg, lam[s.tau1[t]]);
+            const double2 la = s.tau0[t] ? lam1 : lam0, lb = cscale(sg, s.tau1[t] ? lam1 : lam0);
             const double2 p0 = cmul(la, v), p1 = cmul(lb, v);
             a[0] += p0.x;
             a[1] += p0.y;
             a[2] += p1.x;
             a[3] += p1.y;
-            nl[t] = cadd(cmul(m0, la), cmul(m1, lb));
+            Lam[base ^ s.tq[t]] = cadd(cmul(m0, la), cmul(m1, lb));
         }
-        for (int t = 0; t < s.ntq; t++) Lam[base ^ s.tq[t]] = nl[t];
-    }
+    });
     __shared__ double red[4][8];
     __shared__ int last;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
@@ -209,9 +217,12 @@ struct GradEngine {
         cudaSetDevice(prev);
     }
 
+    // a power of two of blocks (grid_cosets splits a coset index into thread and Gray-walk bits), at most maxgrid
     dim3 grid_of(const StepArgs &s) const {
         const uint64_t N = 1ULL << s.nk;
-        return dim3((unsigned)std::max<uint64_t>(1, std::min<uint64_t>((N + 255) / 256, (uint64_t)maxgrid)), (unsigned)bs);
+        uint64_t want = std::max<uint64_t>(1, std::min<uint64_t>((N + 255) / 256, (uint64_t)maxgrid)), gx = 1;
+        while (gx * 2 <= want) gx *= 2;
+        return dim3((unsigned)gx, (unsigned)bs);
     }
     GradCtx ctx() const { return GradCtx{d_M, d_bits, d_item, plan.ns, maxgrid, arena}; }
     size_t seg_per_string() const { return (size_t)std::max(0, every - 1) * seg_stride; }
