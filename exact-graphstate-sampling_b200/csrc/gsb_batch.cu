@@ -126,38 +126,79 @@ __device__ __forceinline__ void team_cosets(const TM &tm, int nk, const uint64_t
     }
 }
 
-// One write pass of step s with bit `bit`, outputs scaled by `scale`; returns the written norm (to every thread).
-template <typename E, typename TM>
-__device__ double team_step(const TM &tm, const BStep &s, const uint64_t *tk, E *arena, int bit, double scale) {
+// One coset of step s: inputs already loaded (v), outputs stored, their squared norm returned.
+template <typename E, typename T, int NTQ>
+__device__ __forceinline__ T coset_out(const BStep &s, E *arena, uint64_t c, uint64_t base, const T (&vr)[NTQ],
+                                       const T (&vi)[NTQ], T m0r, T m0i, T m1r, T m1i) {
+    const int pc = __popcll(c & s.rhoc) & 1;
+    // x = 0 and signed x = 1 sums of the two outputs, in scalars (no runtime-indexed arrays)
+    T a0r = 0, a0i = 0, a1r = 0, a1i = 0, b0r = 0, b0i = 0, b1r = 0, b1i = 0;
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) {
+        T xr = vr[t], xi = vi[t];
+        if (s.tau0[t]) { a1r += xr; a1i += xi; } else { a0r += xr; a0i += xi; }
+        if ((pc ^ s.par[t]) & 1) { xr = -xr; xi = -xi; }
+        if (s.tau1[t]) { b1r += xr; b1i += xi; } else { b0r += xr; b0i += xi; }
+    }
+    const T r0 = m0r * a0r - m0i * a0i + m1r * b0r - m1i * b0i;
+    const T i0 = m0r * a0i + m0i * a0r + m1r * b0i + m1i * b0r;
+    st_e(arena, base, r0, i0);
+    T n = r0 * r0 + i0 * i0;
+    if (s.m == 2) {
+        const T r1 = m0r * a1r - m0i * a1i + m1r * b1r - m1i * b1i;
+        const T i1 = m0r * a1i + m0i * a1r + m1r * b1i + m1i * b1r;
+        st_e(arena, base ^ s.g, r1, i1);
+        n += r1 * r1 + i1 * i1;
+    }
+    return n;
+}
+
+// The write pass over the member's cosets (team_cosets' order), two cosets per iteration: both cosets' inputs are
+// loaded before either's outputs are stored (distinct cosets never share a slot, so this order is safe in place),
+// which doubles the loads in flight of a latency-bound team.
+template <typename E, typename TM, int NTQ>
+__device__ double team_step_n(const TM &tm, const BStep &s, const uint64_t *tk, E *arena, int bit, double scale) {
     typedef typename ArithOf<E>::T T;
     const T m0r = (T)(scale * s.M[4 * bit + 0]), m0i = (T)(scale * s.M[4 * bit + 1]);
     const T m1r = (T)(scale * s.M[4 * bit + 2]), m1i = (T)(scale * s.M[4 * bit + 3]);
     double nb = 0;
-    team_cosets(tm, s.nk, tk, [&](uint64_t c, uint64_t base) {
-        const int pc = __popcll(c & s.rhoc) & 1;
-        // x = 0 and signed x = 1 sums of the two outputs, in scalars (no runtime-indexed arrays)
-        T a0r = 0, a0i = 0, a1r = 0, a1i = 0, b0r = 0, b0i = 0, b1r = 0, b1i = 0;
-        for (int t = 0; t < s.ntq; t++) {
-            T vr, vi;
-            ld_e(arena, base ^ s.tq[t], vr, vi);
-            if (s.tau0[t]) { a1r += vr; a1i += vi; } else { a0r += vr; a0i += vi; }
-            if ((pc ^ s.par[t]) & 1) { vr = -vr; vi = -vi; }
-            if (s.tau1[t]) { b1r += vr; b1i += vi; } else { b0r += vr; b0i += vi; }
+    const int ls = tm.log2size();
+    const uint64_t r = (uint64_t)tm.rank();
+    if (!(s.nk < ls && r >= (1ULL << s.nk))) {
+        const uint64_t lo = bcoset_base(tk, r);
+        const uint64_t nh = s.nk > ls ? 1ULL << (s.nk - ls) : 1;
+        uint64_t hi = 0;
+        for (uint64_t n = 0; n < nh; n += 2) {
+            if (n) hi ^= tk[ls + __ffsll((long long)n) - 1];
+            const uint64_t c0 = r | ((n ^ (n >> 1)) << ls), b0 = lo ^ hi;
+            const bool two = n + 1 < nh;
+            const uint64_t hi1 = two ? hi ^ tk[ls] : hi;              // Gray step n -> n + 1 flips bit 0
+            const uint64_t c1 = r | (((n + 1) ^ ((n + 1) >> 1)) << ls), b1 = lo ^ hi1;
+            T v0r[NTQ], v0i[NTQ], v1r[NTQ], v1i[NTQ];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                ld_e(arena, b0 ^ s.tq[t], v0r[t], v0i[t]);
+                if (two) ld_e(arena, b1 ^ s.tq[t], v1r[t], v1i[t]);
+                else { v1r[t] = 0; v1i[t] = 0; }
+            }
+            T nn = coset_out<E, T, NTQ>(s, arena, c0, b0, v0r, v0i, m0r, m0i, m1r, m1i);
+            if (two) nn += coset_out<E, T, NTQ>(s, arena, c1, b1, v1r, v1i, m0r, m0i, m1r, m1i);
+            nb += (double)nn;
+            hi = hi1;
         }
-        const T r0 = m0r * a0r - m0i * a0i + m1r * b0r - m1i * b0i;
-        const T i0 = m0r * a0i + m0i * a0r + m1r * b0i + m1i * b0r;
-        st_e(arena, base, r0, i0);
-        T n = r0 * r0 + i0 * i0;
-        if (s.m == 2) {
-            const T r1 = m0r * a1r - m0i * a1i + m1r * b1r - m1i * b1i;
-            const T i1 = m0r * a1i + m0i * a1r + m1r * b1i + m1i * b1r;
-            st_e(arena, base ^ s.g, r1, i1);
-            n += r1 * r1 + i1 * i1;
-        }
-        nb += (double)n;
-    });
+    }
     tm.sync();
     return tm.sum(nb);
+}
+
+// One write pass of step s with bit `bit`, outputs scaled by `scale`; returns the written norm (to every thread).
+template <typename E, typename TM>
+__device__ double team_step(const TM &tm, const BStep &s, const uint64_t *tk, E *arena, int bit, double scale) {
+    switch (s.ntq) {
+        case 1: return team_step_n<E, TM, 1>(tm, s, tk, arena, bit, scale);
+        case 2: return team_step_n<E, TM, 2>(tm, s, tk, arena, bit, scale);
+        default: return team_step_n<E, TM, 4>(tm, s, tk, arena, bit, scale);
+    }
 }
 
 // Live table before step s, in (coset, offset) order, to / from a compact buffer.
