@@ -48,19 +48,28 @@ __device__ __forceinline__ void dp_load<float2>(const float2 *p, double &re, dou
 __device__ __forceinline__ void dp_store(double2 *p, double re, double im) { *p = make_double2(re, im); }
 __device__ __forceinline__ void dp_store(float2 *p, double re, double im) { *p = make_float2((float)re, (float)im); }
 
-// w: per vertex (w0re, w0im, w1re, w1im)
+// w: per vertex (w0re, w0im, w1re, w1im).  The grid is a power of two of threads, 2^ls: a thread takes the outputs
+// c' = t | (g << ls) for the Gray codes g of the high bits, so pdep(c', pivmask) is its fixed low part XOR one
+// running value (one XOR per output instead of a loop over the bits of c').
 template <typename E>
 __global__ void k_dp_step(const DpStep s, const E *__restrict__ old, E *__restrict__ nw, const double *__restrict__ w) {
-    const uint64_t N = 1ULL << s.rn;
     const uint64_t low = s.r >= 64 ? ~0ULL : ((1ULL << s.r) - 1), xbit = 1ULL << s.r;
     const double w0r = w[4 * s.v], w0i = w[4 * s.v + 1], w1r = w[4 * s.v + 2], w1i = w[4 * s.v + 3];
-    for (uint64_t cp = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; cp < N; cp += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t u0 = 0;
-        for (int j = 0; j < s.npos; j++)
-            if ((cp >> j) & 1) u0 |= 1ULL << s.pos[j];
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const int ls = __ffsll((long long)nthreads) - 1;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s.rn < ls && t >= (1ULL << s.rn)) return;
+    uint64_t lo = 0;
+    for (int j = 0; j < s.npos && j < ls; j++)
+        if ((t >> j) & 1) lo |= 1ULL << s.pos[j];
+    const uint64_t nh = s.rn > ls ? 1ULL << (s.rn - ls) : 1;
+    uint64_t hi = 0;
+    for (uint64_t n = 0; n < nh; n++) {
+        if (n) hi ^= 1ULL << s.pos[ls + __ffsll((long long)n) - 1];
+        const uint64_t cp = t | ((n ^ (n >> 1)) << ls), u0 = lo ^ hi;
         double ar = 0, ai = 0;
-        for (int t = 0; t < s.nspan; t++) {
-            const uint64_t u = u0 ^ s.span[t], c = u & low;
+        for (int q = 0; q < s.nspan; q++) {
+            const uint64_t u = u0 ^ s.span[q], c = u & low;
             double vr, vi;
             dp_load(old + c, vr, vi);
             double cr, ci;
@@ -77,6 +86,14 @@ __global__ void k_dp_step(const DpStep s, const E *__restrict__ old, E *__restri
         }
         dp_store(nw + cp, ar, ai);
     }
+}
+
+// A power of two of 256-thread blocks covering 2^rn outputs, at most `cap` blocks (k_dp_step's thread split).
+static unsigned dp_grid(int rn, uint64_t cap) {
+    const uint64_t want = std::max<uint64_t>(1, std::min<uint64_t>(((1ULL << rn) + 255) / 256, cap));
+    uint64_t g = 1;
+    while (g * 2 <= want) g *= 2;
+    return (unsigned)g;
 }
 
 template <typename E>
@@ -138,9 +155,7 @@ static cudaError_t dp_enqueue_slice(DpEngine *D) {
     k_dp_begin<E><<<1, 1, 0, D->stream>>>((E *)D->ta);
     E *a = (E *)D->ta, *b = (E *)D->tb;
     for (const DpStep &s : D->st) {
-        const uint64_t N = 1ULL << s.rn;
-        const int grid = (int)std::min<uint64_t>((N + 255) / 256, (uint64_t)D->sms * 8);
-        k_dp_step<E><<<grid, 256, 0, D->stream>>>(s, a, b, D->d_w);
+        k_dp_step<E><<<dp_grid(s.rn, (uint64_t)D->sms * 8), 256, 0, D->stream>>>(s, a, b, D->d_w);
         std::swap(a, b);
     }
     k_dp_accumulate<E><<<1, 1, 0, D->stream>>>(a, D->d_pre, D->d_slice, D->d_acc);
@@ -364,7 +379,7 @@ int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const
     DP_CK(cudaMalloc(&w, 32));
     DP_CK(cudaMemcpy(a, old, na * 16, cudaMemcpyHostToDevice));
     DP_CK(cudaMemcpy(w, wv, 32, cudaMemcpyHostToDevice));
-    k_dp_step<double2><<<(unsigned)std::min<size_t>((nb + 255) / 256, 4096), 256>>>(st, a, b, w);
+    k_dp_step<double2><<<dp_grid(rn, 4096), 256>>>(st, a, b, w);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaMemcpy(out, b, nb * 16, cudaMemcpyDeviceToHost);
     cudaFree(a);
@@ -399,7 +414,7 @@ int gsb_dp_extend_static(int r, int rn, uint64_t rho, uint64_t pivmask, int nker
     const size_t na = (size_t)1 << r, nb = (size_t)1 << rn;
     DP_CK(cudaMemcpy(a, old, na * 16, cudaMemcpyHostToDevice));
     DP_CK(cudaMemcpy(w, wv, 32, cudaMemcpyHostToDevice));
-    k_dp_step<double2><<<(unsigned)std::min<size_t>((nb + 255) / 256, 4096), 256>>>(st, a, b, w);
+    k_dp_step<double2><<<dp_grid(rn, 4096), 256>>>(st, a, b, w);
     DP_CK(cudaGetLastError());
     DP_CK(cudaMemcpy(out, b, nb * 16, cudaMemcpyDeviceToHost));
     return 0;
