@@ -12,6 +12,7 @@
 // A class's outputs land only in its own input slots or in slots no class reads (checked on the host), so tiles are
 // independent and the pass is race-free in place.
 #pragma once
+#include <type_traits>
 #include "gsb_kernels.cuh"
 
 namespace gsb {
@@ -360,7 +361,188 @@ __device__ __forceinline__ void group_cosets(const GroupArgs &ga, const GroupSte
     }
 }
 
-template <typename E, typename T, bool FIRST, bool LAST, bool STS, int NB, int NR>
+// Packed two-lane FP32 (sm_100 add / mul / fma .f32x2): one 64-bit register holds the same quantity for the
+// thread's two adjacent classes.  Each lane rounds exactly like the scalar instruction.
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 f2_pack(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_mul(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// group_cosets for complex64 with FP32 arithmetic, two classes per thread in packed registers: every coset sum,
+// rotation product and norm term of the class pair is one f32x2 instruction.  The stage buffers between the steps of
+// a pass hold a class pair as (re0, re1, im0, im1), so they load and store as one 16-byte access with no shuffles;
+// the arena tile and the arena keep (re, im) per entry.  The class sign multiplies the x = 1 sums (an exact +-1
+// product), so every lane computes what the scalar form computes, in the same order; only the norm's partial sums
+// split over the two lanes.
+template <int NTQ, int H, bool FIRST, bool LAST, bool STS, int NR>
+__device__ __forceinline__ void group_cosets_pk(const GroupArgs &ga, const GroupStepArgs &gs, float2 *__restrict__ mem,
+                                                const uint64_t TB, const int L, const uint32_t (&in)[1],
+                                                const uint32_t (&out)[1][NR], const float (&w_r)[NR][2],
+                                                const float (&w_i)[NR][2], float (&nsum)[1][NR]) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr bool ANY = H < 0;
+    const uint32_t NC = 1u << L;
+    const int LG = L - 1;   // log2 class pairs per tile
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const int m = ANY ? gs.m : 2;
+    const int ntq = ANY ? gs.ntq : NTQ;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    f32x2 sg[NTQ];
+    int ta0[NTQ], ta1[NTQ];
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) {
+        const float s = gs.par[t] ? -1.f : 1.f;
+        sg[t] = f2_pack(s, s);
+        ta0[t] = ANY ? gs.tau0[t] : (t < NTQ - H ? 0 : 1);
+        ta1[t] = ANY ? gs.tau1[t] : 1 - ta0[t];
+    }
+    // M rows, both lanes equal: re, im and -im of M[r][0] and M[r][1]
+    f32x2 W0R[NR], W0I[NR], W0N[NR], W1R[NR], W1I[NR], W1N[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        W0R[r] = f2_pack(w_r[r][0], w_r[r][0]);
+        W0I[r] = f2_pack(w_i[r][0], w_i[r][0]);
+        W0N[r] = f2_pack(-w_i[r][0], -w_i[r][0]);
+        W1R[r] = f2_pack(w_r[r][1], w_r[r][1]);
+        W1I[r] = f2_pack(w_i[r][1], w_i[r][1]);
+        W1N[r] = f2_pack(-w_i[r][1], -w_i[r][1]);
+    }
+    // class signs of a pair (p even): class p + 1 differs from class p by parity(lambda & 1)
+    const float sig1 = (lam & 1u) ? -1.f : 1.f;
+    const f32x2 SGP = f2_pack(1.f, sig1), SGN = f2_pack(-1.f, -sig1);
+    f32x2 NS[NR];
+#pragma unroll
+    for (int r = 0; r < NR; r++) NS[r] = 0ull;
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t zl[NTQ], ib[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            ib[t] = t < ntq ? (uint32_t)gs.in_idx[j][t] * NC : 0u;
+            zl[t] = FIRST && t < ntq ? ga.z0lo[j][t] : 0u;
+        }
+        uint32_t ol[2] = {0, 0}, oidx[2] = {0, 0};
+        float2 *ob[2] = {mem, mem};
+#pragma unroll
+        for (int tau = 0; tau < 2; tau++) {
+            oidx[tau] = tau < m ? (uint32_t)gs.out_idx[j][tau] * NC : 0u;
+            ol[tau] = LAST && tau < m ? ga.zdlo[j][tau] : 0u;
+            if (LAST && tau < m) ob[tau] = mem + (TB ^ ga.blk_out[gs.out_idx[j][tau]]);
+        }
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = 2u * g;
+            f32x2 X0R[2] = {0ull, 0ull}, X0I[2] = {0ull, 0ull}, X1R[2] = {0ull, 0ull}, X1I[2] = {0ull, 0ull};
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                if (t >= ntq) continue;
+                f32x2 VR, VI;
+                if (FIRST) {
+                    const float2 *src = reinterpret_cast<const float2 *>(smem + in[0]) + ib[t];
+                    const uint32_t pos = pc ^ zl[t];
+                    const float2 a = src[pos], b = src[pos ^ 1u];
+                    VR = f2_pack(a.x, b.x);
+                    VI = f2_pack(a.y, b.y);
+                } else {
+                    const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in[0]) + (ib[t] + pc));
+                    VR = f2_pack(v.x, v.y);
+                    VI = f2_pack(v.z, v.w);
+                }
+                if (ANY) {
+                    if (ta0[t]) { X0R[1] = f2_add(X0R[1], VR); X0I[1] = f2_add(X0I[1], VI); }
+                    else { X0R[0] = f2_add(X0R[0], VR); X0I[0] = f2_add(X0I[0], VI); }
+                    if (ta1[t]) { X1R[1] = f2_fma(sg[t], VR, X1R[1]); X1I[1] = f2_fma(sg[t], VI, X1I[1]); }
+                    else { X1R[0] = f2_fma(sg[t], VR, X1R[0]); X1I[0] = f2_fma(sg[t], VI, X1I[0]); }
+                } else {
+                    X0R[ta0[t]] = f2_add(X0R[ta0[t]], VR);
+                    X0I[ta0[t]] = f2_add(X0I[ta0[t]], VI);
+                    X1R[ta1[t]] = f2_fma(sg[t], VR, X1R[ta1[t]]);
+                    X1I[ta1[t]] = f2_fma(sg[t], VI, X1I[ta1[t]]);
+                }
+            }
+            const f32x2 SG = ((mp ^ __popc(pc & lam)) & 1) ? SGN : SGP;
+#pragma unroll
+            for (int tau = 0; tau < 2; tau++) {
+                if (tau >= m) continue;
+                const bool h0 = ANY || (tau == 0 ? NTQ - H > 0 : H > 0);
+                const bool h1 = ANY || (tau == 0 ? H > 0 : NTQ - H > 0);
+                f32x2 ZR = 0ull, ZI = 0ull;
+                if (h1) {
+                    ZR = f2_mul(SG, X1R[tau]);
+                    ZI = f2_mul(SG, X1I[tau]);
+                }
+#pragma unroll
+                for (int r = 0; r < NR; r++) {
+                    f32x2 RE = 0ull, IM = 0ull;
+                    if (h0) {
+                        RE = f2_mul(W0R[r], X0R[tau]);
+                        RE = f2_fma(W0N[r], X0I[tau], RE);
+                        IM = f2_mul(W0R[r], X0I[tau]);
+                        IM = f2_fma(W0I[r], X0R[tau], IM);
+                    }
+                    if (h1) {
+                        RE = h0 ? f2_fma(W1R[r], ZR, RE) : f2_mul(W1R[r], ZR);
+                        RE = f2_fma(W1N[r], ZI, RE);
+                        IM = h0 ? f2_fma(W1R[r], ZI, IM) : f2_mul(W1R[r], ZI);
+                        IM = f2_fma(W1I[r], ZR, IM);
+                    }
+                    NS[r] = f2_fma(RE, RE, NS[r]);
+                    NS[r] = f2_fma(IM, IM, NS[r]);
+                    if (LAST || STS) {
+                        float r0, r1, i0, i1;
+                        f2_unpack(RE, r0, r1);
+                        f2_unpack(IM, i0, i1);
+                        if (LAST) {
+                            const uint32_t pos = pc ^ ol[tau];
+                            ob[tau][pos] = make_float2(r0, i0);
+                            ob[tau][pos ^ 1u] = make_float2(r1, i1);
+                        }
+                        if (STS)
+                            *reinterpret_cast<float4 *>(reinterpret_cast<float2 *>(smem + out[0][r]) + (oidx[tau] + pc)) =
+                                make_float4(r0, r1, i0, i1);
+                    }
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+        float a, b;
+        f2_unpack(NS[r], a, b);
+        nsum[0][r] += a + b;
+    }
+}
+
+template <typename E, typename T, bool FIRST, bool LAST, bool STS, int NB, int NR, bool PK>
 __device__ __forceinline__ void group_cosets_any(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
                                                  const uint64_t TB, const int L, const uint32_t (&in)[NB],
                                                  const uint32_t (&out)[NB][NR], const T (&w_r)[NR][2],
@@ -368,18 +550,35 @@ __device__ __forceinline__ void group_cosets_any(const GroupArgs &ga, const Grou
     // classes per thread: two adjacent classes for complex64 (their values sit in one 16-byte span of a block),
     // one for complex128.  Four per thread was measured slower: per-class 8-byte accesses at a 32-byte stride
     // conflict in shared memory and scatter the arena stores.
+    // PK (FP32 arithmetic only): the packed form, with its stage layout, for every step of the pass.
     constexpr int P = sizeof(E) == 8 ? 2 : 1;
-#define GSB_GC(NTQ_, H_) group_cosets<E, T, P, NTQ_, H_, FIRST, LAST, STS, NB, NR>(ga, gs, mem, TB, L, in, out, w_r, w_i, ns)
-    switch (gs.kind) {   // uniform across the grid
-        case GK_1_0: GSB_GC(1, 0); break;
-        case GK_2_0: GSB_GC(2, 0); break;
-        case GK_2_1: GSB_GC(2, 1); break;
-        case GK_4_0: GSB_GC(4, 0); break;
-        case GK_4_1: GSB_GC(4, 1); break;
-        case GK_4_2: GSB_GC(4, 2); break;
-        default: GSB_GC(4, -1); break;
-    }
+    if constexpr (PK) {
+        static_assert(std::is_same<T, float>::value, "packed form: FP32 arithmetic");
+        static_assert(NB == 1 && sizeof(E) == 8, "packed form: one complex64 table");
+#define GSB_GC(NTQ_, H_) group_cosets_pk<NTQ_, H_, FIRST, LAST, STS, NR>(ga, gs, mem, TB, L, in, out, w_r, w_i, ns)
+        switch (gs.kind) {   // uniform across the grid
+            case GK_1_0: GSB_GC(1, 0); break;
+            case GK_2_0: GSB_GC(2, 0); break;
+            case GK_2_1: GSB_GC(2, 1); break;
+            case GK_4_0: GSB_GC(4, 0); break;
+            case GK_4_1: GSB_GC(4, 1); break;
+            case GK_4_2: GSB_GC(4, 2); break;
+            default: GSB_GC(4, -1); break;
+        }
 #undef GSB_GC
+    } else {
+#define GSB_GC(NTQ_, H_) group_cosets<E, T, P, NTQ_, H_, FIRST, LAST, STS, NB, NR>(ga, gs, mem, TB, L, in, out, w_r, w_i, ns)
+        switch (gs.kind) {
+            case GK_1_0: GSB_GC(1, 0); break;
+            case GK_2_0: GSB_GC(2, 0); break;
+            case GK_2_1: GSB_GC(2, 1); break;
+            case GK_4_0: GSB_GC(4, 0); break;
+            case GK_4_1: GSB_GC(4, 1); break;
+            case GK_4_2: GSB_GC(4, 2); break;
+            default: GSB_GC(4, -1); break;
+        }
+#undef GSB_GC
+    }
 }
 
 // Bits of a sampling pass ('sample' / 'prob': the normalised two-pass chain, gsamp2.cpp:39-55), decided at the start
@@ -531,6 +730,10 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
     __syncthreads();
     if (!s_ok) return;
     const GroupSmem sm = group_smem<E, T, D, TR>(ga.ssz, L);
+    // Packed FP32 pairs pay where a trailing step evaluates both branch rows on the same coset sums (the sampling
+    // passes, 3-7 % faster per pass).  A packed instruction holds the FMA pipe for two cycles, so passes without a
+    // trailing step gain no throughput from it and lost up to 10 % to the extra register moves: they stay scalar.
+    constexpr bool PK = std::is_same<T, float>::value && TR == 1;
     const uint32_t bar0 = smem_addr(smem);
     // per-step M row of the step's bit; the first step carries the pass's scale
     T w[D][1][2], wj[D][1][2];
@@ -612,10 +815,10 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
         // written steps: the first reads the input tile, the last writes the arena (and keeps its stage for the
         // trailing step); the input buffer is free once the first step is done: tile it + 2 goes there
         if (D == 1) {
-            group_cosets_any<E, T, true, true, TR == 1, 1, 1>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
+            group_cosets_any<E, T, true, true, TR == 1, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         } else {
-            group_cosets_any<E, T, true, false, true, 1, 1>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
+            group_cosets_any<E, T, true, false, true, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         }
         if (threadIdx.x == 0 && it + 2 < i1 && !ga.withhold_loads) {
@@ -623,16 +826,16 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             issued++;
         }
         if (D == 2) {
-            group_cosets_any<E, T, false, true, TR == 1, 1, 1>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
+            group_cosets_any<E, T, false, true, TR == 1, 1, 1, PK>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
         } else if (D == 3) {
-            group_cosets_any<E, T, false, false, true, 1, 1>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
+            group_cosets_any<E, T, false, false, true, 1, 1, PK>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
             __syncthreads();
-            group_cosets_any<E, T, false, true, false, 1, 1>(ga, ga.st[2], mem, TB, L, m2, none1, w[2], wj[2], ns[2]);
+            group_cosets_any<E, T, false, true, false, 1, 1, PK>(ga, ga.st[2], mem, TB, L, m2, none1, w[2], wj[2], ns[2]);
         }
         if (TR) {
             if (D > 1) __syncthreads();
             const uint32_t(&tmid)[1] = D == 1 ? m1 : m2;
-            group_cosets_any<E, T, false, false, false, 1, 2>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
+            group_cosets_any<E, T, false, false, false, 1, 2, PK>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
         }
         __syncthreads();
 #pragma unroll
