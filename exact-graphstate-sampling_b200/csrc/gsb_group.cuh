@@ -780,18 +780,17 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
         mbar_init_fence();
     }
     __syncthreads();
-    auto issue_loads = [&](unsigned int n) {   // tile n into buffer (n - i0) & 1
+    auto issue_loads = [&](unsigned int n, uint64_t TBn) {   // tile n (base TBn) into buffer (n - i0) & 1
         const int buf = (int)((n - i0) & 1);
         const uint32_t bar = bar0 + 8 * (uint32_t)buf;
         const uint32_t dst = bar0 + sm.in0 + (uint32_t)buf * sm.in_bytes;
-        const uint64_t TBn = tile_tb(n);
         mbar_arrive_expect_tx(bar, sm.in_bytes);
         for (int i = 0; i < ga.ssz[0]; i++) bulk_load(dst + (uint32_t)i * blk_bytes, mem + (TBn ^ ga.blk_in[i]), blk_bytes, bar);
     };
     int issued = 0;   // tiles whose loads thread 0 issued
     if (threadIdx.x == 0 && !ga.withhold_loads)
         for (unsigned int n = i0; n < i1 && n < i0 + 2; n++) {
-            issue_loads(n);
+            issue_loads(n, tile_tb(n));
             issued++;
         }
     int waited = 0;   // tiles whose loads completed
@@ -822,7 +821,10 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             __syncthreads();
         }
         if (threadIdx.x == 0 && it + 2 < i1 && !ga.withhold_loads) {
-            issue_loads(it + 2);
+            // tile it + 2 is two Gray-code steps from this tile (gray(n + 1) = gray(n) ^ 2^ctz(n + 1)); rebuilding its
+            // base from the index, a loop over the class-base vectors, held up warp 0 and so every warp at the next
+            // barrier (4-7 % of the pass)
+            issue_loads(it + 2, TB ^ ((ga.bhi[__ffs((int)(it + 1)) - 1] ^ ga.bhi[__ffs((int)(it + 2)) - 1]) & ~mask));
             issued++;
         }
         if (D == 2) {
