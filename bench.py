@@ -46,7 +46,7 @@ import replicas  # noqa: E402  (package module: torchrun rank bookkeeping)
 
 METRIC = "s/sample & amps/s at n=70 w=30, c64 form vs c128 plain, |Δlog2P|≤1e-5; HBM GB/s"
 WORKLOAD = "matching_n70_d70_s2_w30"
-K_GROUP_TRAFFIC_RATIO = 0.9722
+K_GROUP_TRAFFIC_RATIO = 0.9726
 
 
 def parse():
