@@ -1415,6 +1415,30 @@ int gsb_sample_groups(const gsb_engine *e, int *group_len, double *entries) {
     return 0;
 }
 
+int gsb_pass_list(const gsb_engine *e, int mode, int cap, int *k0, int *d, int *tr, int *fused, int *count) {
+    if (!e || !count || cap < 0 || (mode != 0 && mode != 1)) return fail(GSB_E_USAGE, "bad argument");
+    if (cap > 0 && (!k0 || !d || !tr || !fused)) return fail(GSB_E_USAGE, "null argument");
+    const Engine *E = eng(e);
+    const std::vector<Op> &ops = mode == 0 ? E->chain_ops : E->sample_ops;
+    int n = 0;
+    auto put = [&](int a, int b, int c, int f) {
+        if (n < cap) {
+            k0[n] = a;
+            d[n] = b;
+            tr[n] = c;
+            fused[n] = f;
+        }
+        n++;
+    };
+    if (ops.empty()) {   // no fusion: one pass per step
+        for (int k = 0; k < E->plan.ns; k++) put(k, 1, 0, 0);
+    } else {
+        for (const Op &op : ops) put(op.k0, op.group ? op.d : 1, op.group ? op.tr : 0, op.group ? 1 : 0);
+    }
+    *count = n;
+    return 0;
+}
+
 int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries) {
     if (!e || !group_len) return fail(GSB_E_USAGE, "null argument");
     const Engine *E = eng(e);

@@ -75,6 +75,8 @@ def _load():
         "gsb_grad_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_grad_run": (c.c_int, [P, dp, c.POINTER(c.c_int8), c.c_int64, dp, dp]),
         "gsb_sample_groups": (c.c_int, [P, c.POINTER(c.c_int), dp]),
+        "gsb_pass_list": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int),
+                                    c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_test_withhold_tile_loads": (c.c_int, [P, c.c_int]),
         "gsb_autotune": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_batch_open": (c.c_int, [c.POINTER(c.c_char_p), c.POINTER(c.c_size_t), c.c_int, c.c_int, c.c_int,
@@ -103,7 +105,7 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_test_withhold_tile_loads", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_test_withhold_tile_loads", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
            "gsb_grad_run", "gsb_autotune", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
@@ -337,6 +339,16 @@ class Engine:
         e = np.zeros(max(self.ns, 1), np.float64)
         _check(_lib.gsb_sample_groups(self.handle, _ptr(g, ctypes.c_int), _ptr(e, ctypes.c_double)))
         return [int(x) for x in g[:self.ns]], e[:self.ns]
+
+    def passes(self, mode=0):
+        """The passes of 'chain' (mode 0) or 'prob' / 'sample' (mode 1) in launch order: a list of
+        (first step, steps written, trailing branch-norm step 0/1, fused 0/1)."""
+        n = ctypes.c_int()
+        _check(_lib.gsb_pass_list(self.handle, int(mode), 0, None, None, None, None, ctypes.byref(n)))
+        cols = [np.zeros(max(n.value, 1), np.int32) for _ in range(4)]
+        _check(_lib.gsb_pass_list(self.handle, int(mode), n.value, *[_ptr(a, ctypes.c_int) for a in cols],
+                                  ctypes.byref(n)))
+        return [tuple(int(a[i]) for a in cols) for i in range(n.value)]
 
     def set_arith(self, bits):
         """complex64 wide-step arithmetic: 32 (FP32 sums and rotation, default) or 64 (exact sums + FP64 rotation,

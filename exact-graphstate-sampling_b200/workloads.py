@@ -118,6 +118,30 @@ def graph_state_instance(n=20, p=0.5, seed=1, order_seed=11, iters=20000):
     return dict(name=f"gnp_n{n}_s{seed}", n=n, body=body, tail=tail, order=order, width=R, plan=text, steps=st)
 
 
+def twin_graph_instance(h=46, ntw=14, seed=10, p=0.5, order_seed=11, iters=8000):
+    """Graph state of a G(h, p) graph plus ntw false twins (a copy of a vertex's neighbourhood), then a seeded U3 per
+    qubit.  Measuring a twin after its original can leave the step with one output class (m = 1): the defaults give
+    such a step at cut rank 14 (k = 35, width 19), wide enough for the fused passes' generic dataflow path."""
+    rng = np.random.default_rng(seed)
+    n = h + ntw
+    E = {(i, j) for i in range(h) for j in range(i + 1, h) if rng.random() < p}
+    for t, v in enumerate(rng.choice(h, ntw, replace=False)):
+        w = h + t
+        for (a, b) in list(E):
+            if a == v and b < h:
+                E.add((min(b, w), max(b, w)))
+            if b == v and a < h:
+                E.add((min(a, w), max(a, w)))
+    body = [("h", [q]) for q in range(n)] + [("cz", [a, b]) for (a, b) in sorted(E)]
+    tail = [circuits.u3_op(q, *(float(x) for x in rng.uniform(0, 2 * np.pi, 3))) for q in range(n)]
+    from graphform import graph_form
+    A, _ = graph_form(circuits.tableau_of(n, body))
+    order, w = gsb.order_search(A, seed=order_seed, ngreedy=4, iters=iters)
+    text, st, R = build(n, body, tail, order)
+    return dict(name=f"twins_h{h}_t{ntw}_s{seed}", n=n, body=body, tail=tail, order=order, width=R, plan=text,
+                steps=st)
+
+
 def pass_bytes(steps, esize, passes="chain"):
     """Algorithmic bytes of one string: a write pass moves E (2^{r_k} + 2^{r_{k+1}}), a norm pass E 2^{r_k}
     (r_{k+1} = nk + log2 m).  passes: 'chain' (write only) or 'sample' (norm + write per step)."""

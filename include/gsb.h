@@ -130,6 +130,12 @@ int gsb_fusion_groups(const gsb_engine *e, int *group_len, double *entries);
 /* The same for the sampling passes ('prob' / 'sample'): group_len[k] = steps written by the pass starting at step k;
  * entries[k] = table entries it reads plus writes, including the norm pass launched before it where it has one. */
 int gsb_sample_groups(const gsb_engine *e, int *group_len, double *entries);
+/* The passes of one mode (0 'chain', 1 'prob' / 'sample') in launch order: pass i starts at step k0[i], writes d[i]
+ * steps, also evaluates the branch norms of step k0[i] + d[i] when tr[i] = 1, and is a fused k_group pass when
+ * fused[i] = 1 (otherwise a single-step pass, after its own norm pass in sampling mode).  *count receives the number
+ * of passes; at most cap entries are written (the arrays may be NULL when cap = 0).  No counterpart in the reference:
+ * it shows this executor's pass lists (as built, autotuned or set by gsb_set_fusion). */
+int gsb_pass_list(const gsb_engine *e, int mode, int cap, int *k0, int *d, int *tr, int *fused, int *count);
 /* Replace every step's rotation matrix: M is [nsteps][2][2] complex (re, im), M[k][b][x] as the plan text lists
  * it.  The layout stays; this is how one engine (one arena) serves all slice plans of make_sliced_plans, which
  * share the layout and differ only in M (sliced_plans.py:1-14). */

@@ -1,6 +1,7 @@
 """Parity of the wide-step kernels (steps of >= 2^10 / 2^11 cosets: the complex128 kernel and the complex64 paired
-kernel) with the oracle, in every executor mode, on an instance wide enough to use them; and complex128 amplitudes
-against a brute-force statevector at n = 24.
+kernel) and of the fused passes with the oracle, in every executor mode, on instances wide enough to use them (one of
+them with a wide single-output step, the fused passes' generic dataflow shape); and complex128 amplitudes against a
+brute-force statevector at n = 24.
 
 Modes: "c128" (complex128 arena), "c64x" (complex64 arena, exact pair sums + FP64 rotation: the oracle's own
 complex64 arithmetic) and "c64" (complex64 arena, FP32 arithmetic, the default).  Tolerances: c128 |d log2 Pr| <=
@@ -201,3 +202,54 @@ def test_fused_chain_depths_vs_oracle(wide_case, mode):
         eng.set_matrices_from_text(open(wide_case["path"]).read())
         assert eng.fusion_groups()[0] == tuned
         assert np.array_equal(eng.chain(strings)[0], lp)
+
+
+@pytest.fixture(scope="module")
+def twin_case():
+    import workloads
+    w = workloads.twin_graph_instance()
+    w["m1"] = [k for k, s in enumerate(w["steps"]) if s["m"] == 1 and s["r"] >= 12]
+    assert w["m1"], "the twin instance must keep a wide one-output step"
+    td = tempfile.mkdtemp()
+    path = os.path.join(td, "plan.txt")
+    open(path, "w").write(w["plan"])
+    w["path"] = path
+    return w
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_fused_one_output_step_vs_oracle(twin_case, mode):
+    """A wide step with a single output class (m = 1: a twin vertex measured after its original) runs the fused
+    passes' generic dataflow shape (GK_ANY): in 'chain' passes at depths 2 and 3, and in the sampling passes both as a
+    written step and as the trailing branch-norm step (the packed FP32 form in mode "c64").  The pass lists must
+    cover it that way, and chain, prob and sample must give the oracle's results."""
+    import workloads
+    from oracle import Oracle
+    ns = n = len(twin_case["steps"])
+    m1 = twin_case["m1"]
+    strings = workloads.random_strings(ns, 8, seed=3)
+    o = Oracle(twin_case["path"], 128 if mode == "c128" else 64)
+    ref = [o.chain1(s) for s in strings]
+    sref = [o.sample(0, 9, i) for i in range(4)]
+    o.close()
+    in_chain = in_written = in_trailing = False
+    with engine(twin_case["path"], mode) as eng:
+        for depth in (2, 3):
+            eng.set_fusion(depth)
+            for k0, d, tr, fused in eng.passes(0):
+                in_chain |= bool(fused) and d >= 2 and any(k0 <= k < k0 + d for k in m1)
+            for k0, d, tr, fused in eng.passes(1):
+                in_written |= bool(fused) and any(k0 <= k < k0 + d for k in m1)
+                in_trailing |= bool(fused and tr) and (k0 + d) in m1
+            lp, cond = eng.chain(strings)
+            lpp = eng.prob(strings)
+            bits, slp = eng.sample(4, 9)
+            for i, (olp, ocond) in enumerate(ref):
+                assert abs(lp[i] - olp) <= lp_tol(mode, olp, n), (depth, i, lp[i], olp)
+                assert abs(lpp[i] - olp) <= lp_tol(mode, olp, n), (depth, i, lpp[i], olp)
+                if olp > -n - 3:
+                    assert np.abs(cond[i] - ocond).max() <= cond_tol(mode), depth
+            for i in range(4):
+                ob, olp = sref[i]
+                assert list(bits[i]) == list(ob) and abs(slp[i] - olp) <= lp_tol(mode, olp, n), (depth, i)
+    assert in_chain and in_written and in_trailing, (in_chain, in_written, in_trailing)
