@@ -447,6 +447,7 @@ def run_form_batch(args):
         snap = 1 << st[K]["r"]
         byt += 16 * E * (pre + 4 * suf + 2 * snap + 3 * 2 * snap)
     peak, kind = peaks()
+    l2 = max(gsb.probe_l2_copy(mib=mib) for mib in (16, 24, 32))
     _form_line("batch", "amps/s, 512 instances n in [16,40] x 64 strings, one persistent launch", nstr / (ms / 1e3),
                "amps/s", True, {
                    "ms_per_launch": ms, "strings": int(nstr), "instances": len(plans),
@@ -458,6 +459,10 @@ def run_form_batch(args):
                    "roofline": {"bound": "hbm", "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
                                 "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
                                 "note": "team tables <= 2^20 entries: many items are L2-resident"},
+                   "roofline_l2": {"bound": "l2", "achieved": byt / (ms / 1e3) / 1e9, "peak": l2, "unit": "GB/s",
+                                   "frac": byt / (ms / 1e3) / 1e9 / l2,
+                                   "peak_kind": "measured here: L2 copy bandwidth (gsb_probe_l2_copy, best of "
+                                                "16/24/32 MiB buffers, one launch of 400 passes)"},
                    "host_planning_s": t_plan, "steps": args.steps, "warmup": args.warmup,
                })
 

@@ -19,7 +19,7 @@ CLI128 = os.path.join(HERE, "gsb2_c128")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
-LIB_SOURCES = ["gsb_engine.cu", "gsb_dp.cu", "gsb_grad.cu", "gsb_batch.cu", "gsb_plan.cpp", "gsb_order.cpp", "gsb_fuse.cpp"]
+LIB_SOURCES = ["gsb_engine.cu", "gsb_dp.cu", "gsb_grad.cu", "gsb_batch.cu", "gsb_probe.cu", "gsb_plan.cpp", "gsb_order.cpp", "gsb_fuse.cpp"]
 LIB_DEPS = LIB_SOURCES + ["gsb_kernels.cuh", "gsb_group.cuh", "gsb_step.h", "gsb_plan.h", "gsb_common.h", "gsb_fuse.h"]
 
 

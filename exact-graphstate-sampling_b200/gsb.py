@@ -75,6 +75,7 @@ def _load():
         "gsb_grad_info": (c.c_int, [P, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_grad_run": (c.c_int, [P, dp, c.POINTER(c.c_int8), c.c_int64, dp, dp]),
         "gsb_sample_groups": (c.c_int, [P, c.POINTER(c.c_int), dp]),
+        "gsb_probe_l2_copy": (c.c_int, [c.c_int, c.c_uint64, c.c_int, c.POINTER(c.c_float)]),
         "gsb_pass_list": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int),
                                     c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_test_withhold_tile_loads": (c.c_int, [P, c.c_int]),
@@ -105,7 +106,7 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_test_withhold_tile_loads", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_probe_l2_copy", "gsb_test_withhold_tile_loads", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
            "gsb_grad_run", "gsb_autotune", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
@@ -532,6 +533,14 @@ def dp_extend(old, r, rn, rho, piv, ker, wv, device=0):
 def dp_extend_static(old, r, rn, rho, piv, ker, wv, device=0):
     """dp_extend without device allocation (static scratch in the library; r, rn <= 16; calls must not overlap)."""
     return _extend(_lib.gsb_dp_extend_static, old, r, rn, rho, piv, ker, wv, device)
+
+
+def probe_l2_copy(device=0, mib=24, reps=400):
+    """L2 copy bandwidth of a device (GB/s, bytes read + written): one launch copies an L2-resident buffer of `mib`
+    MiB onto another `reps` times.  The denominator of the L2 roofline of L2-resident work."""
+    g = ctypes.c_float()
+    _check(_lib.gsb_probe_l2_copy(int(device), int(mib) << 20, int(reps), ctypes.byref(g)))
+    return float(g.value)
 
 
 def validate_text(text):

@@ -136,6 +136,10 @@ int gsb_sample_groups(const gsb_engine *e, int *group_len, double *entries);
  * of passes; at most cap entries are written (the arrays may be NULL when cap = 0).  No counterpart in the reference:
  * it shows this executor's pass lists (as built, autotuned or set by gsb_set_fusion). */
 int gsb_pass_list(const gsb_engine *e, int mode, int cap, int *k0, int *d, int *tr, int *fused, int *count);
+/* L2 copy bandwidth of a device in GB/s (bytes read + written): one launch copies an L2-resident buffer of `bytes`
+ * (1-64 MiB, a multiple of 16) onto another `reps` times.  The denominator of the L2 roofline reported for the
+ * batched launch, whose team tables stay in L2.  No counterpart in the reference (a measurement aid). */
+int gsb_probe_l2_copy(int device, uint64_t bytes, int reps, float *gbs);
 /* Replace every step's rotation matrix: M is [nsteps][2][2] complex (re, im), M[k][b][x] as the plan text lists
  * it.  The layout stays; this is how one engine (one arena) serves all slice plans of make_sliced_plans, which
  * share the layout and differ only in M (sliced_plans.py:1-14). */
