@@ -80,3 +80,10 @@ def test_batch_single_prefix_single_suffix_and_longest_prefix():
         with gsb.Engine.from_text(w["plan"], precision=gsb.GSB_C128) as eng:
             want = eng.chain(np.concatenate([pre[i][0], suf[i][0, 0]])[None, :])[0][0]
         assert abs(lp[i, 0, 0] - want) <= 1e-9 or (not np.isfinite(want) and not np.isfinite(lp[i, 0, 0]))
+
+
+def test_l2_probe_measures_a_copy_bandwidth():
+    """The L2 roofline's denominator: copying an L2-resident 24 MiB buffer runs well above HBM speed."""
+    import gsb
+    gbs = gsb.probe_l2_copy(mib=24, reps=100)
+    assert 2000.0 < gbs < 1e6, gbs

@@ -96,3 +96,15 @@ def test_clifford_group_and_circuits():
         assert np.allclose(W.conj().T @ W, np.eye(2), atol=1e-14)
     with pytest.raises(ValueError):
         amp.tail_matrix([("ry(0.3)", [0])])
+
+
+def test_l2_probe_rejects_bad_sizes():
+    """gsb_probe_l2_copy checks its arguments before touching a device: buffers of 1-64 MiB, 1-100000 passes."""
+    import gsb
+    for kw in (dict(mib=0), dict(mib=65), dict(mib=16, reps=0)):
+        try:
+            gsb.probe_l2_copy(**kw)
+        except gsb.GsbError as e:
+            assert e.code == 1, kw
+        else:
+            raise AssertionError(f"accepted {kw}")
