@@ -494,7 +494,16 @@ def run_form_grad(args):
         if i >= max(3, args.warmup):
             times.append(time.perf_counter() - t0)
     t = statistics.median(times)
+    # algorithmic bytes of the sweep (complex128): per string, every step's forward pass twice (the sweep and the
+    # recompute of its checkpoint segment: read 2^r, write 2^r') and its reverse pass (read the step's input table and
+    # lambda_{k+1}, write lambda_k: 2^r + 2^r' + 2^r); the time is the whole loss + gradient, host work included
+    fwd = sum((1 << s["r"]) + (1 << s["rn"]) for s in w["steps"])
+    bwd = sum(2 * (1 << s["r"]) + (1 << s["rn"]) for s in w["steps"])
+    byt = 16.0 * len(bits) * (2 * fwd + bwd)
+    peak, kind = peaks()
     _form_line("grad", "s per loss+gradient, n=48 rotation layer, 2048 exact targets", t, "s", False, {
+        "roofline": {"bound": "hbm", "achieved": byt / t / 1e9, "peak": peak, "unit": "GB/s", "frac": byt / t / 1e9 / peak,
+                     "peak_kind": kind, "bytes_per_string": byt / len(bits)},
         "strings_per_s": len(bits) / t, "loss": loss.item(), "grad_norm": float(theta.grad.norm()),
         "width": w["width"], "checkpoint_every": 4, "dtype": "c128 arena, f64",
         "targets": "2048 exact samples of a second seeded n=48 instance (complex128 executor)",

@@ -67,6 +67,25 @@ __device__ __forceinline__ void grid_cosets(const StepArgs &s, F f) {
     }
 }
 
+// The same walk, two consecutive Gray-code cosets per call: f(c0, base0, c1, base1, two), the second only when two.
+template <typename F>
+__device__ __forceinline__ void grid_cosets2(const StepArgs &s, F f) {
+    const uint64_t nthreads = (uint64_t)gridDim.x * blockDim.x;
+    const int ls = __ffsll((long long)nthreads) - 1;
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s.nk < ls && t >= (1ULL << s.nk)) return;
+    const uint64_t lo = coset_base(s, t);
+    const uint64_t nh = s.nk > ls ? 1ULL << (s.nk - ls) : 1;
+    uint64_t hi = 0;
+    for (uint64_t n = 0; n < nh; n += 2) {
+        if (n) hi ^= s.tk[ls + __ffsll((long long)n) - 1];
+        const bool two = n + 1 < nh;
+        const uint64_t hi1 = two ? hi ^ s.tk[ls] : hi;   // Gray step n -> n + 1 flips high bit 0
+        f(t | ((n ^ (n >> 1)) << ls), lo ^ hi, t | (((n + 1) ^ ((n + 1) >> 1)) << ls), lo ^ hi1, two);
+        hi = hi1;
+    }
+}
+
 __device__ __forceinline__ void step_row(const StepArgs &s, const GradCtx &g, double2 &m0, double2 &m1) {
     const int b = g.bits[(size_t)(*g.item + (int)blockIdx.y) * (size_t)g.ns + (size_t)s.k];
     const double *Mk = g.M + (size_t)s.k * 8 + 4 * b;
@@ -83,26 +102,39 @@ __device__ __forceinline__ double2 cscale(double s, double2 a) { return make_dou
 __global__ void k_gr_begin(double2 *T, const GradCtx g) { T[blockIdx.y * g.arena] = make_double2(1.0, 0.0); }
 
 // Forward step on the T arena: gathers the input table to `gather` ([c][t], if given) and, if `write`, stores the
-// step's outputs in place.
+// step's outputs in place.  Two cosets per iteration, both cosets' loads first (distinct cosets never share a slot),
+// so a thread has twice the loads in flight (7 % off the sweep); NTQ (the step's offsets) is a template parameter, so
+// the loaded values stay in registers.
+template <int NTQ>
 __global__ void __launch_bounds__(256) k_gr_fwd(const StepArgs s, double2 *__restrict__ T, double2 *__restrict__ gather,
                                                 size_t gather_stride, int write, const GradCtx g) {
     double2 m0, m1;
     step_row(s, g, m0, m1);
     T += blockIdx.y * g.arena;
     if (gather) gather += blockIdx.y * gather_stride;
-    grid_cosets(s, [&](uint64_t c, uint64_t base) {
+    auto one = [&](uint64_t c, uint64_t base, const double2 (&v)[NTQ]) {
         const int pc = __popcll(c & s.rhoc) & 1;
         double2 o0 = make_double2(0, 0), o1 = make_double2(0, 0);   // scalars: no runtime-indexed arrays
-        for (int t = 0; t < s.ntq; t++) {
-            const double2 v = T[base ^ s.tq[t]];
-            if (gather) gather[c * (uint64_t)s.ntq + (uint64_t)t] = v;
-            const double2 a = cmul(m0, v), b = cscale((pc ^ s.par[t]) ? -1.0 : 1.0, cmul(m1, v));
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            if (gather) gather[c * (uint64_t)NTQ + (uint64_t)t] = v[t];
+            const double2 a = cmul(m0, v[t]), b = cscale((pc ^ s.par[t]) ? -1.0 : 1.0, cmul(m1, v[t]));
             if (s.tau0[t]) o1 = cadd(o1, a); else o0 = cadd(o0, a);
             if (s.tau1[t]) o1 = cadd(o1, b); else o0 = cadd(o0, b);
         }
         if (!write) return;
         T[base] = o0;
         if (s.m == 2) T[base ^ s.g] = o1;
+    };
+    grid_cosets2(s, [&](uint64_t c0, uint64_t b0, uint64_t c1, uint64_t b1, bool two) {
+        double2 v0[NTQ], v1[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            v0[t] = T[b0 ^ s.tq[t]];
+            v1[t] = two ? T[b1 ^ s.tq[t]] : make_double2(0, 0);
+        }
+        one(c0, b0, v0);
+        if (two) one(c1, b1, v1);
     });
 }
 
@@ -128,6 +160,7 @@ __global__ void k_gr_set_item(int *item, int v) { *item = v; }
 // Reverse step: lambda_{k+1} (output slots of the Lam arena) -> lambda_k (input slots, in place), and
 // dZ/dM_k[b_k][x] from the step's input table Tk ([c][t]).  Deterministic reduction: per-block partials, the last
 // block sums them in block order and writes grad[item][k] = (dZ/dm0, dZ/dm1).
+template <int NTQ>
 __global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 *__restrict__ Tk, size_t tk_stride,
                                                 double2 *__restrict__ Lam, const GradCtx g, double *partials,
                                                 unsigned int *counter, double *grad) {
@@ -138,20 +171,34 @@ __global__ void __launch_bounds__(256) k_gr_bwd(const StepArgs s, const double2 
     partials += (size_t)blockIdx.y * 4 * (size_t)g.maxgrid;
     counter += blockIdx.y;
     double a[4] = {0, 0, 0, 0};   // dZ/dm0 (re, im), dZ/dm1 (re, im)
-    grid_cosets(s, [&](uint64_t c, uint64_t base) {
+    // two cosets per iteration: both cosets' lambda and input values are read before either writes (a coset writes
+    // only its own slots)
+    auto one = [&](uint64_t c, uint64_t base, double2 lam0, double2 lam1, const double2 (&v)[NTQ]) {
         const int pc = __popcll(c & s.rhoc) & 1;
-        const double2 lam0 = Lam[base], lam1 = s.m == 2 ? Lam[base ^ s.g] : make_double2(0, 0);   // read first
-        for (int t = 0; t < s.ntq; t++) {
-            const double2 v = Tk[c * (uint64_t)s.ntq + (uint64_t)t];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
             const double sg = (pc ^ s.par[t]) ? -1.0 : 1.0;
             const double2 la = s.tau0[t] ? lam1 : lam0, lb = cscale(sg, s.tau1[t] ? lam1 : lam0);
-            const double2 p0 = cmul(la, v), p1 = cmul(lb, v);
+            const double2 p0 = cmul(la, v[t]), p1 = cmul(lb, v[t]);
             a[0] += p0.x;
             a[1] += p0.y;
             a[2] += p1.x;
             a[3] += p1.y;
             Lam[base ^ s.tq[t]] = cadd(cmul(m0, la), cmul(m1, lb));
         }
+    };
+    grid_cosets2(s, [&](uint64_t c0, uint64_t b0, uint64_t c1, uint64_t b1, bool two) {
+        const double2 z = make_double2(0, 0);
+        const double2 l00 = Lam[b0], l01 = s.m == 2 ? Lam[b0 ^ s.g] : z;
+        const double2 l10 = two ? Lam[b1] : z, l11 = two && s.m == 2 ? Lam[b1 ^ s.g] : z;
+        double2 v0[NTQ], v1[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            v0[t] = Tk[c0 * (uint64_t)NTQ + (uint64_t)t];
+            v1[t] = two ? Tk[c1 * (uint64_t)NTQ + (uint64_t)t] : z;
+        }
+        one(c0, b0, l00, l01, v0);
+        if (two) one(c1, b1, l10, l11, v1);
     });
     __shared__ double red[4][8];
     __shared__ int last;
@@ -239,6 +286,18 @@ struct GradEngine {
     size_t seg_per_string() const { return (size_t)std::max(0, every - 1) * seg_stride; }
     double2 *seg(int pos) const { return d_seg + (size_t)(pos - 1) * seg_stride; }   // pos = 1 .. every-1 (slot 0)
 
+    // forward / reverse step launches, instantiated for the step's number of coset offsets
+    void fwd(const StepArgs &s, double2 *gather, size_t gstride, int write, const GradCtx &g) {
+        if (s.ntq == 1) k_gr_fwd<1><<<grid_of(s), 256, 0, stream>>>(s, T, gather, gstride, write, g);
+        else if (s.ntq == 2) k_gr_fwd<2><<<grid_of(s), 256, 0, stream>>>(s, T, gather, gstride, write, g);
+        else k_gr_fwd<4><<<grid_of(s), 256, 0, stream>>>(s, T, gather, gstride, write, g);
+    }
+    void bwd(const StepArgs &s, const double2 *tk, size_t tstride, const GradCtx &g) {
+        if (s.ntq == 1) k_gr_bwd<1><<<grid_of(s), 256, 0, stream>>>(s, tk, tstride, Lam, g, partials, d_counter, d_grad);
+        else if (s.ntq == 2) k_gr_bwd<2><<<grid_of(s), 256, 0, stream>>>(s, tk, tstride, Lam, g, partials, d_counter, d_grad);
+        else k_gr_bwd<4><<<grid_of(s), 256, 0, stream>>>(s, tk, tstride, Lam, g, partials, d_counter, d_grad);
+    }
+
     // The sequence of one launch of bs strings (captured once as a graph).
     cudaError_t enqueue() {
         const int ns = plan.ns;
@@ -247,8 +306,7 @@ struct GradEngine {
         k_gr_begin<<<one, 1, 0, stream>>>(T, g);
         for (int k = 0; k < ns; k++) {
             const StepArgs &s = args[(size_t)k];
-            k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, k % every == 0 ? d_ckpt + ckpt_off[(size_t)k] : nullptr,
-                                                    ckpt_n, 1, g);
+            fwd(s, k % every == 0 ? d_ckpt + ckpt_off[(size_t)k] : nullptr, ckpt_n, 1, g);
         }
         k_gr_final<<<one, 1, 0, stream>>>(T, Lam, d_z, g);
         for (int c = ((ns - 1) / every) * every; c >= 0; c -= every) {
@@ -258,14 +316,12 @@ struct GradEngine {
             for (int j = c; j < e; j++) {   // recompute: gather T_j (j > c), write T_{j+1} (j < e - 1)
                 if (j == c && e - 1 == c) break;
                 const StepArgs &s = args[(size_t)j];
-                k_gr_fwd<<<grid_of(s), 256, 0, stream>>>(s, T, j == c ? nullptr : seg(j - c), seg_per_string(),
-                                                        j < e - 1 ? 1 : 0, g);
+                fwd(s, j == c ? nullptr : seg(j - c), seg_per_string(), j < e - 1 ? 1 : 0, g);
             }
             for (int j = e - 1; j >= c; j--) {
                 const StepArgs &s = args[(size_t)j];
                 const double2 *tk = j == c ? d_ckpt + ckpt_off[(size_t)c] : seg(j - c);
-                k_gr_bwd<<<grid_of(s), 256, 0, stream>>>(s, tk, j == c ? ckpt_n : seg_per_string(), Lam, g, partials,
-                                                        d_counter, d_grad);
+                bwd(s, tk, j == c ? ckpt_n : seg_per_string(), g);
             }
         }
         k_gr_next<<<1, 1, 0, stream>>>(d_item, bs);
