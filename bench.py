@@ -531,6 +531,8 @@ def run_form_wide34(args):
         t2 = time.perf_counter()
         sbits, slp = eng.sample(16, seed=7)
         t_smp = time.perf_counter() - t2
+        chain_bytes = 8.0 * float(eng.fusion_groups()[1].sum())     # bytes the executed passes move per string
+        sample_bytes = 8.0 * float(eng.sample_groups()[1].sum())
     # complex128 cross-check of 4 amplitudes: a second order with 3 slice vertices cut out (width 33), every slice's
     # final table from 'prefix', summed by 'resume' (the reference's slicing identity)
     t3 = time.perf_counter()
@@ -557,6 +559,11 @@ def run_form_wide34(args):
         "log2p_first": [float(x) for x in lp[:4]], "sample_log2p": [float(x) for x in slp[:4]],
         "dtype": "c64 arena, f32 sums, f64 norms/scales", "host_planning_s": t_plan,
         "timing": "wall clock around the host-buffer C-ABI calls (whole batches, one synchronisation each)",
+        "roofline": {"bound": "hbm", "achieved": 256 * chain_bytes / t_amp / 1e9, "peak": peaks()[0], "unit": "GB/s",
+                     "frac": 256 * chain_bytes / t_amp / 1e9 / peaks()[0], "peak_kind": peaks()[1],
+                     "pass_bytes_per_string": chain_bytes, "sample_pass_bytes": sample_bytes,
+                     "sample_achieved": 16 * sample_bytes / t_smp / 1e9,
+                     "note": "wall clock (host calls included), so a lower bound on the kernels' rate"},
         "c128_sliced_check": {"slices": len(sl["plans"]), "slice_vertices": sl["S"], "width": sl["width"],
                               "arena_gb": (1 << sl["width"]) * 16 / 1e9,
                               "log2p_c64_vs_c128": check,
