@@ -505,6 +505,7 @@ def run_form_grad(args):
         "roofline": {"bound": "hbm", "achieved": byt / t / 1e9, "peak": peak, "unit": "GB/s", "frac": byt / t / 1e9 / peak,
                      "peak_kind": kind, "bytes_per_string": byt / len(bits)},
         "strings_per_s": len(bits) / t, "loss": loss.item(), "grad_norm": float(theta.grad.norm()),
+        "step_times_s": [round(x, 4) for x in times],
         "width": w["width"], "checkpoint_every": 4, "dtype": "c128 arena, f64",
         "targets": "2048 exact samples of a second seeded n=48 instance (complex128 executor)",
         "steps": args.steps, "warmup": max(3, args.warmup)})
