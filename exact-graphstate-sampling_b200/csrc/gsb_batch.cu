@@ -642,10 +642,18 @@ int gsb_batch_run(gsb_batch *h, double *log2p, float *ms) {
     return 0;
 }
 
+// The largest block the batch kernel of this precision can launch with (its registers per thread bound it), or 0.
+static int batch_max_block(const BatchEngine &E) {
+    cudaFuncAttributes fa{};
+    const cudaError_t e = E.prec == 128 ? cudaFuncGetAttributes(&fa, k_batch<double2>) : cudaFuncGetAttributes(&fa, k_batch<float2>);
+    return e == cudaSuccess ? fa.maxThreadsPerBlock : 0;
+}
+
 int gsb_batch_set_shape(gsb_batch *h, int block, int small_R, int per_sm) {
     if (!h || (block != 64 && block != 128 && block != 256 && block != 512 && block != 1024) || small_R < 0 ||
         small_R > 24 || per_sm < 1 || per_sm > 16 || block * per_sm > 2048)
         return fail(GSB_E_USAGE, "bad shape");
+    if (block > batch_max_block(h->E)) return fail(GSB_E_USAGE, "block larger than the batch kernel can launch");
     h->E.shape = BatchShape{block, small_R, per_sm};
     return 0;
 }
@@ -668,10 +676,11 @@ int gsb_batch_tune(gsb_batch *h, int reps, size_t max_bytes, int *block, int *sm
     float best = 1e30f;
     BatchShape bs = E.shape;
     const int maxR = E.max_R();
+    const int max_block = batch_max_block(E);   // shapes the kernel cannot launch are skipped
     for (int blk : {128, 256, 512})
         for (int sr : {0, 8, 10, 12, 14})
             for (int ps : {1, 2, 4}) {
-                if (blk * ps > 2048 || sr > maxR + 1) continue;
+                if (blk * ps > 2048 || sr > maxR + 1 || blk > max_block) continue;
                 BatchShape sh{blk, sr, ps};
                 std::vector<int> big, small;
                 int bR, sR, grid;

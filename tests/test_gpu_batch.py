@@ -82,6 +82,23 @@ def test_batch_single_prefix_single_suffix_and_longest_prefix():
         assert abs(lp[i, 0, 0] - want) <= 1e-9 or (not np.isfinite(want) and not np.isfinite(lp[i, 0, 0]))
 
 
+def test_batch_rejects_shapes_it_cannot_launch():
+    """A block larger than the batch kernel's register budget allows is refused up front (a usage error), and the
+    autotuner only tries shapes that launch, in both precisions."""
+    import gsb
+    import workloads
+    bw = workloads.batch_workload(count=4, seed=3, nmin=16, nmax=20, npre=2, nsuf=2, iters=2000)
+    for prec in (gsb.GSB_C64, gsb.GSB_C128):
+        b = gsb.Batch([w["plan"] for w in bw["instances"]], precision=prec)
+        b.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+        with pytest.raises(gsb.GsbError) as e:
+            b.set_shape(1024, 12, 1)
+        assert e.value.code == 1
+        block, small_R, per_sm, ms = b.tune(reps=1)
+        assert block <= 512 and ms > 0
+        b.run()
+
+
 def test_l2_probe_measures_a_copy_bandwidth():
     """The L2 roofline's denominator: copying an L2-resident 24 MiB buffer runs well above HBM speed."""
     import gsb
