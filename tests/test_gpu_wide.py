@@ -253,3 +253,22 @@ def test_fused_one_output_step_vs_oracle(twin_case, mode):
                 ob, olp = sref[i]
                 assert list(bits[i]) == list(ob) and abs(slp[i] - olp) <= lp_tol(mode, olp, n), (depth, i)
     assert in_chain and in_written and in_trailing, (in_chain, in_written, in_trailing)
+
+
+def test_pass_lists_cover_every_step_once(wide_case):
+    """gsb_pass_list: both modes' passes cover the steps in order, each once, agree with the group lengths that
+    gsb_fusion_groups / gsb_sample_groups report, and only fused passes carry a trailing branch-norm step."""
+    ns = len(wide_case["steps"])
+    with engine(wide_case["path"], "c64") as eng:
+        for depth in (1, 2, 3):
+            eng.set_fusion(depth)
+            for mode, groups in ((0, eng.fusion_groups), (1, eng.sample_groups)):
+                passes = eng.passes(mode)
+                glen, _ = groups()
+                k = 0
+                for k0, d, tr, fused in passes:
+                    assert k0 == k and d >= 1 and (fused or (d == 1 and tr == 0)), (mode, depth, k0, d, tr, fused)
+                    assert glen[k0] == d and (tr == 0 or k0 + d < ns), (mode, depth, k0)
+                    k += d
+                assert k == ns, (mode, depth)
+                assert mode == 1 or all(tr == 0 for _, _, tr, _ in passes)
