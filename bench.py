@@ -47,6 +47,8 @@ import replicas  # noqa: E402  (package module: torchrun rank bookkeeping)
 METRIC = "s/sample & amps/s at n=70 w=30, c64 form vs c128 plain, |Δlog2P|≤1e-5; HBM GB/s"
 WORKLOAD = "matching_n70_d70_s2_w30"
 K_GROUP_TRAFFIC_RATIO = 0.9726
+# the headline workload's plan text (tests/golden/make_headline_plan.py writes it; a host test pins it to the package)
+HEADLINE_PLAN = os.path.join(ROOT, "tests", "golden", "headline", "matching_n70_w30_plan.txt")
 
 
 def parse():
@@ -60,6 +62,10 @@ def parse():
     ap.add_argument("--c128-amps", type=int, default=8)
     ap.add_argument("--c128-samples", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-plan", default=HEADLINE_PLAN,
+                    help="--impl reference: plan file to time (default: the committed headline plan)")
+    ap.add_argument("--ref-samples", type=int, default=2,
+                    help="--impl reference: exact samples drawn by the reference executor for s/sample (0 = none)")
     ap.add_argument("--arith", type=int, default=32, choices=[32, 64],
                     help="arithmetic of the complex64 wide-step kernels (32: FP32; 64: exact sums + FP64 rotation)")
     ap.add_argument("--fusion", type=int, default=2, choices=[1, 2, 3],
@@ -151,56 +157,92 @@ class Clocks:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def ref_chain_time(plan_path, strings_path, threads):
-    """Wall time of the reference executor ('chain' mode, complex64) on the strings file, and its stdout."""
+def ref_time(plan_path, mode_args, threads, precision=64):
+    """Wall time and stdout of the reference executor (oracle/_ref/gsamp2, compiled from the reference's sources)
+    on `gsamp2 <plan> <mode_args...>`; without that build, the C restatement of the same executor ('port')."""
     from oracle import ref_binary, run_ref
     t0 = time.perf_counter()
-    if ref_binary(64):
-        out = run_ref(64, [plan_path, "chain", strings_path], threads=threads)
-        kind = "reference"
-    else:
-        from oracle import Oracle
-        o = Oracle(plan_path, 64)
-        out = ""
-        for ln in open(strings_path):
+    if ref_binary(precision):
+        out = run_ref(precision, [plan_path] + list(mode_args), threads=threads)
+        return time.perf_counter() - t0, out, "reference"
+    from oracle import Oracle
+    o = Oracle(plan_path, precision)
+    lines = []
+    if mode_args[0] == "chain":
+        for ln in open(mode_args[1]):
             if ln.strip():
                 lp, _ = o.chain1(ln.strip())
-                out += f"{lp:.12f}\n"
-        kind = "port"
-    return time.perf_counter() - t0, out, kind
+                lines.append(f"{lp:.12f}")
+    else:                                                    # sample N seed
+        for i in range(int(mode_args[1])):
+            bits, lp = o.sample(0, int(mode_args[2]), i)
+            lines.append("".join(map(str, bits)) + f" {lp:.12f}")
+    o.close()
+    return time.perf_counter() - t0, "\n".join(lines) + "\n", "port"
+
+
+def repo_libraries():
+    """Shared objects of this repository mapped into this process (from /proc/self/maps), relative paths."""
+    root = os.path.realpath(ROOT) + os.sep
+    seen = set()
+    try:
+        for ln in open("/proc/self/maps"):
+            f = ln.split()
+            if len(f) >= 6 and (f[-1].endswith(".so") or ".so." in f[-1]):
+                p = os.path.realpath(f[-1])
+                if p.startswith(root):
+                    seen.add(os.path.relpath(p, root))
+    except OSError:
+        pass
+    return sorted(seen)
 
 
 def run_reference(args):
+    """The reference's own CPU executor on the headline workload, every host thread, rank 0 only.  The plan comes
+    from a committed file, so this process loads nothing of this repository's package or library."""
     if int(os.environ.get("RANK", "0")) != 0:   # rank 0 alone times the host reference; no process group needed
         return
-    import workloads
-    w = workloads.matching_n70_w30()
+    import numpy as np
+    from oracle import ref_isa
+    plan_text = open(args.ref_plan).read()
+    head = plan_text.split(None, 3)
+    n, ns, width = int(head[0]), int(head[1]), int(head[2])
     cores = os.cpu_count() or 1
-    strings = workloads.random_strings(len(w["steps"]), args.warmup + args.steps, seed=4242)
+    strings = np.random.default_rng(4242).integers(0, 2, size=(args.warmup + args.steps, ns), dtype=np.int8)
     with tempfile.TemporaryDirectory() as td:
         plan = os.path.join(td, "plan.txt")
-        open(plan, "w").write(w["plan"])
+        open(plan, "w").write(plan_text)
         times = []
         kind = "reference"
         for i in range(args.warmup + args.steps):
             sp = os.path.join(td, f"s{i}.txt")
             open(sp, "w").write("".join(str(int(b)) for b in strings[i]) + "\n")
-            t, _, kind = ref_chain_time(plan, sp, cores)
+            t, _, kind = ref_time(plan, ["chain", sp], cores)
             if i >= args.warmup:
                 times.append(t)
+        samples = {}
+        if args.ref_samples > 0:
+            t, out, _ = ref_time(plan, ["sample", str(args.ref_samples), "2000000"], cores)
+            samples = {"s_per_sample": t / args.ref_samples, "samples_per_s": args.ref_samples / t,
+                       "samples_timed": args.ref_samples,
+                       "sample_mode": f"gsamp2 sample {args.ref_samples} 2000000 (one process, wall clock)"}
     tot = sum(times)
     v = args.steps / tot
-    print(json.dumps({
+    isa = ref_isa(64) if kind == "reference" else None
+    line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "amps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1000 * tot / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "c64 arena, f64 arithmetic", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "n": 70, "width": w["width"], "strings_per_step": 1, "mode": "chain",
-                   "l2": "arena 8.6 GB >> L2"},
+        "config": {"workload": WORKLOAD if args.ref_plan == HEADLINE_PLAN else os.path.basename(args.ref_plan),
+                   "n": n, "width": width, "strings_per_step": 1, "mode": "chain", "l2": "arena 8.6 GB >> L2"},
         "cpu_baseline": {"value": v, "unit": "amps/s", "cores": cores, "kind": kind,
                          "sample": f"{args.steps} uniform random strings of the workload, one per step, gsamp2 chain "
-                                   f"mode, OMP_NUM_THREADS={cores}"},
+                                   f"mode, OMP_NUM_THREADS={cores}" + (f", built -march=x86-64-{isa}" if isa else "")},
         "e2e": {"value": v, "unit": "amps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }), flush=True)
+        "repo_libraries_loaded": repo_libraries(),
+    }
+    line.update(samples)
+    print(json.dumps(line), flush=True)
 
 
 def run_gsb(args):
@@ -390,7 +432,7 @@ def run_gsb(args):
             sp = os.path.join(td, "s.txt")
             open(sp, "w").write("".join(str(int(b)) for b in strings[W * A]) + "\n")
             cores = os.cpu_count() or 1
-            t, txt, kind = ref_chain_time(plan, sp, cores)
+            t, txt, kind = ref_time(plan, ["chain", sp], cores)
             ref_lp = float(txt.split()[0])
             out["cpu_baseline"] = {"value": 1.0 / t, "unit": "amps/s", "cores": cores, "kind": kind,
                                    "sample": "1 uniform random string of the workload, gsamp2 chain mode (complex64)",

@@ -8,12 +8,15 @@ Drop-in for the reference's ``engine.py``:
   GPU engine (libgsb ``gsb_dp_*``) in process on the same plan and jobs files.  The result is the same list of
   complex amplitudes (sum over slices of prefactor * Z).
 """
-import itertools
 import os
 
 import numpy as np
 
 from plan import plan
+
+
+def _parity(x):
+    return bin(x).count("1") & 1
 
 
 def write_plan(path, steps, m):
@@ -27,40 +30,43 @@ def write_plan(path, steps, m):
 
 
 class Sliced:
-    """Z(w) for graph A with the vertices in S summed outside the DP (graph A - S inside)."""
+    """Z(w) of graph A with the vertices S summed outside the DP; the DP runs on the induced graph of the others.
+
+    For an assignment a of the slice vertices,
+        Z = sum_a  prod_{v in S} w_v(a_v) * (-1)^{a^T A[S, S]_< a} * Z_{A - S}(w^a),
+    where w^a_q keeps w_q(0) and multiplies w_q(1) by (-1)^{<A[q, S], a>}.  Both signs are parities of bitmasks over
+    the assignment index (bit s-1-i of the index is a_{S[i]}, so indices 0 .. 2^s-1 follow the reference's
+    assignment order and its jobs file byte for byte)."""
 
     def __init__(self, A, order, S):
-        n = len(A)
-        self.S = list(S)
-        Sset = set(S)
-        self.keep = [q for q in order if q not in Sset]
-        self.idx = {q: i for i, q in enumerate(self.keep)}
-        m = len(self.keep)
-        Ak = np.zeros((m, m), np.uint8)
-        for i, p in enumerate(self.keep):
-            for j, q in enumerate(self.keep):
-                Ak[i, j] = A[p, q]
+        A = np.asarray(A)
         self.A = A
-        self.m = m
-        self.n = n
-        self.steps = plan(Ak, list(range(m)))
+        self.n = len(A)
+        self.S = list(S)
+        inS = set(self.S)
+        self.keep = [q for q in order if q not in inS]
+        self.idx = {q: i for i, q in enumerate(self.keep)}
+        self.m = len(self.keep)
+        self.steps = plan(np.ascontiguousarray(A[np.ix_(self.keep, self.keep)], np.uint8), list(range(self.m)))
+        s = len(self.S)
+        self._bit = [1 << (s - 1 - i) for i in range(s)]
+        # kept vertex q: the slice positions it is adjacent to; slice position i: the later slice positions it meets
+        self._cross = [sum(b for b, v in zip(self._bit, self.S) if A[q, v]) for q in self.keep]
+        self._inner = [sum(self._bit[j] for j in range(i + 1, s) if A[self.S[i], self.S[j]]) for i in range(s)]
 
     def slices(self, w):
         """(prefactor, weights of the kept vertices) for every assignment of the sliced vertices."""
-        A, S = self.A, self.S
-        for xs in itertools.product((0, 1), repeat=len(S)):
+        S, bit = self.S, self._bit
+        for a in range(1 << len(S)):
             pre = 1 + 0j
             ph = 0
-            for a, (v, xv) in enumerate(zip(S, xs)):
-                pre *= w[v][xv]
-                for v2, x2 in list(zip(S, xs))[a + 1:]:
-                    ph ^= int(A[v, v2]) & xv & x2
-            pre *= (-1) ** ph
-            ww = []
-            for q in self.keep:
-                f = sum(int(A[q, v]) & xv for v, xv in zip(S, xs)) & 1
-                ww.append((w[q][0], -w[q][1] if f else w[q][1]))
-            yield pre, ww
+            for i, v in enumerate(S):
+                on = 1 if a & bit[i] else 0
+                pre *= w[v][on]
+                if on:
+                    ph ^= _parity(self._inner[i] & a)
+            pre *= -1 if ph else 1
+            yield pre, [(w[q][0], -w[q][1] if _parity(mk & a) else w[q][1]) for q, mk in zip(self.keep, self._cross)]
 
 
 def write_jobs(path, sl, ws):

@@ -19,17 +19,51 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
 
+# the reference checkout: $GSB_REFERENCE_DIR, else the sibling directory "reference" of this repository's checkout
+REF_SRC = os.environ.get("GSB_REFERENCE_DIR",
+                         os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
+_AVX512 = ("avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl")
+
+
 def build(with_ref=None):
     subprocess.run(["make", "-s", "-C", HERE, "all"], check=True)
-    ref_src = os.environ.get("GSB_REFERENCE_DIR", "/root/reference")
     if with_ref is None:
-        with_ref = os.path.exists(os.path.join(ref_src, "gsamp2.cpp"))
+        with_ref = os.path.exists(os.path.join(REF_SRC, "gsamp2.cpp"))
     if with_ref:
-        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_src}"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={os.path.abspath(REF_SRC)}"], check=True)
 
 
-def ref_binary(precision=64):
-    p = os.path.join(REF_DIR, "gsamp2_c128" if precision == 128 else "gsamp2")
+def host_has_avx512():
+    """True when this host's CPU has the x86-64-v4 extensions (AVX-512 F, BW, CD, DQ, VL)."""
+    try:
+        for ln in open("/proc/cpuinfo"):
+            if ln.startswith("flags"):
+                fl = set(ln.split(":", 1)[1].split())
+                return all(f in fl for f in _AVX512)
+    except OSError:
+        pass
+    return False
+
+
+def ref_binary(precision=64, isa=None):
+    """Path of the compiled reference executor (None when not built).  isa: "v4" (AVX-512), "v3" (AVX2), or None
+    for the best level this host runs."""
+    base = "gsamp2_c128" if precision == 128 else "gsamp2"
+    if isa is None:
+        isa = "v4" if host_has_avx512() and os.path.exists(os.path.join(REF_DIR, base + "_v4")) else "v3"
+    p = os.path.join(REF_DIR, base + ("_v4" if isa == "v4" else ""))
+    return p if os.path.exists(p) else None
+
+
+def ref_isa(precision=64):
+    """The instruction-set level ref_binary(precision) picks on this host ("v4" or "v3")."""
+    p = ref_binary(precision)
+    return "v4" if p and p.endswith("_v4") else "v3"
+
+
+def ref_gpu_binary():
+    """Path of the reference's own GPU port (gsamp_cuda.cu built for sm_100a), or None."""
+    p = os.path.join(REF_DIR, "gsamp_cuda")
     return p if os.path.exists(p) else None
 
 

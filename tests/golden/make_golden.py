@@ -1,7 +1,8 @@
 """Generate the golden fixtures of this directory from the reference implementation.
 
-    python tests/golden/make_golden.py            (needs the reference checkout at $GSB_REFERENCE_DIR,
-                                                    default /root/reference, and `make -C oracle ref`)
+    python tests/golden/make_golden.py            (needs the reference checkout at $GSB_REFERENCE_DIR, by default
+                                                    the sibling directory "reference" of this checkout, and
+                                                    `make -C oracle ref`)
     python tests/golden/make_golden.py --w30      (slow: the reference executor on the width-30 gate strings)
 
 Three phases, each in its own process so the reference's flat module names (tableau, plan, amp, ...) never mix
@@ -37,7 +38,7 @@ import tempfile
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 PKG = os.path.join(ROOT, "exact-graphstate-sampling_b200")
-REF = os.environ.get("GSB_REFERENCE_DIR", "/root/reference")
+REF = os.environ.get("GSB_REFERENCE_DIR", os.path.join(os.path.dirname(ROOT), "reference"))
 GATES = ["h", "s", "sdg", "sx", "sxdg", "x", "z", "cz", "cz", "cz"]
 TH = 0.9553166181245092
 
