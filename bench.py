@@ -59,8 +59,14 @@ def parse():
     ap.add_argument("--impl", default="gsb", choices=["gsb", "reference"])
     ap.add_argument("--amps-per-step", type=int, default=16)
     ap.add_argument("--samples", type=int, default=16)
-    ap.add_argument("--c128-amps", type=int, default=8)
-    ap.add_argument("--c128-samples", type=int, default=4)
+    ap.add_argument("--c128-amps", type=int, default=16,
+                    help="strings timed for the complex128 amplitudes/s (every timed string is checked against it)")
+    ap.add_argument("--no-c128", dest="c128", action="store_false")
+    ap.add_argument("--tol", type=float, default=1e-5, help="|d log2 Pr| the complex64 form is held to")
+    ap.add_argument("--no-guard", dest="guard", action="store_false",
+                    help="complex64 without the complex128 re-evaluation of unlikely strings")
+    ap.add_argument("--no-ref-gpu-port", dest="ref_gpu_port", action="store_false",
+                    help="skip timing the reference's own GPU port (oracle/_ref/gsamp_cuda)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-plan", default=HEADLINE_PLAN,
                     help="--impl reference: plan file to time (default: the committed headline plan)")
@@ -76,9 +82,12 @@ def parse():
     ap.add_argument("--profile-mode", default="chain", choices=["chain", "sample"],
                     help="with --profile-chain: evaluate strings (chain) or draw exact samples (sample)")
     ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 128])
-    ap.add_argument("--form", default="headline", choices=["headline", "batch", "grad", "wide34"],
+    ap.add_argument("--proposals", type=int, default=128, help="--form hybrid: proposals per timed run")
+    ap.add_argument("--form", default="headline", choices=["headline", "batch", "grad", "wide34", "hybrid"],
                     help="workload to measure (the default line is the headline n = 70, width-30 workload)")
     ap.add_argument("--batch-instances", type=int, default=512)
+    ap.add_argument("--batch-order", default="qubit", choices=["qubit", "search"],
+                    help="--form batch: qubit index order (widths 7-20, the configuration's) or the native search")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the byte-model pass lists (skip the guarded autotuner)")
     return ap.parse_args()
@@ -245,6 +254,33 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def ref_gpu_port_time(plan_path, strings, ns):
+    """The reference's own GPU port (gsamp_cuda.cu built for sm_100a into oracle/_ref) in 'chain' mode on the first
+    strings of the workload: seconds per string from two runs (1 string and len(strings) strings, so its start-up and
+    arena allocation cancel), and its log2 Pr.  None when that build is absent."""
+    from oracle import ref_gpu_binary
+    exe = ref_gpu_binary()
+    if not exe:
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        def run(k):
+            sp = os.path.join(td, f"s{k}.txt")
+            open(sp, "w").write("".join("".join(str(int(b)) for b in strings[i]) + "\n" for i in range(k)))
+            t0 = time.perf_counter()
+            out = subprocess.run([exe, plan_path, "chain", sp], capture_output=True, text=True, timeout=600)
+            t = time.perf_counter() - t0
+            if out.returncode:
+                raise RuntimeError(f"gsamp_cuda exit {out.returncode}: {out.stderr[-300:]}")
+            return t, [float(ln.split()[0]) for ln in out.stdout.split("\n") if ln.strip()]
+        k = len(strings)
+        t1, _ = run(1)
+        tk, lp = run(k)
+    per = (tk - t1) / (k - 1)
+    return {"s_per_string": per, "amps_per_s": 1.0 / per, "strings_timed": k,
+            "timing": f"wall clock of gsamp_cuda chain on {k} strings minus 1 string (start-up and arena set-up "
+                      f"cancel)", "log2p": lp}
+
+
 def run_gsb(args):
     import numpy as np
     import torch
@@ -261,11 +297,20 @@ def run_gsb(args):
     eng = gsb.Engine.from_text(w["plan"], precision=64, device=local)
     eng.set_arith(args.arith)
     eng.set_fusion(args.fusion)
+    e128 = gsb.Engine.from_text(w["plan"], precision=128, device=local)
+    e128.set_fusion(args.fusion)
     # guarded autotuner of the pass lists (kept only where a whole item gets faster), outside every timed region
     tune64 = eng.autotune(mode=2, reps=3) if args.autotune else None
-    stream = torch.cuda.Stream()                  # a real stream: the engine's kernels and the events share it
+    tune128 = e128.autotune(mode=2, reps=3) if args.autotune else None
+    stream = torch.cuda.Stream()                  # a real stream: the engines' kernels and the events share it
     torch.cuda.set_stream(stream)
     eng.set_stream(stream.cuda_stream)
+    e128.set_stream(stream.cuda_stream)
+    # the complex64 form: complex64 arena, FP32 arithmetic, complex128 re-evaluation of the strings whose complex64
+    # probability lies below the error model's threshold for |d log2 Pr| <= TOL
+    lx = gsb.c64_guard_log2_xmin(ns, args.tol) if args.guard else float("-inf")
+    if args.guard:
+        eng.set_guard(e128, lx)
     strings = workloads.random_strings(ns, (W + K) * A, seed=1000 + rank)
     d_bits = torch.from_numpy(strings).to("cuda")
     d_lp = torch.empty((W + K) * A, dtype=torch.float64, device="cuda")
@@ -281,6 +326,7 @@ def run_gsb(args):
     replicas.barrier(world)
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0 = eng.guard_evaluations()
     with Clocks(local) as clk:
         ev0.record(stream)
         for i in range(W, W + K):
@@ -289,11 +335,11 @@ def run_gsb(args):
         torch.cuda.synchronize()
     replicas.barrier(world)
     torch.cuda.synchronize()
+    guarded_timed = eng.guard_evaluations() - g0
     ms = ev0.elapsed_time(ev1)
     ms_max = replicas.max_over_ranks(ms, world)
     value = world * K * A / (ms_max / 1000.0)
     lp64 = d_lp.cpu().numpy()
-    cond64 = d_cond.cpu().numpy()
 
     # e2e: host strings (pinned) -> C ABI -> host results, every step
     pinned = torch.from_numpy(strings[W * A:(W + K) * A].copy()).pin_memory()
@@ -308,7 +354,7 @@ def run_gsb(args):
     e2e = {"value": world * K * A / e2e_s, "unit": "amps/s", "h2d_bytes_per_step": A * ns,
            "d2h_bytes_per_step": A * 8 + A * ns * 8}
 
-    # exact samples (two passes per DP step), device-resident uniforms
+    # exact samples (fused sampling passes), device-resident uniforms, guarded like the amplitudes
     S = args.samples
     rng = np.random.default_rng(77 + rank)
     d_u = torch.from_numpy(rng.random((S, ns))).to("cuda")
@@ -323,10 +369,26 @@ def run_gsb(args):
     torch.cuda.synchronize()
     s_per_sample64 = replicas.max_over_ranks(e0.elapsed_time(e1) / 1000.0 / S, world)
     sbits64 = d_sb.cpu().numpy()
+    slp64 = d_slp.cpu().numpy()
 
-    # roofline of the dominant kernels (the chain-mode passes: fused groups k_group and single steps), timed per
-    # pass with CUDA events; bytes = the table entries each executed pass must read and write (fused groups keep
-    # their intermediate tables in shared memory, so they move fewer bytes than the unfused step model)
+    # unguarded complex64 on the same strings (its raw error), and a step-timed unguarded batch for the roofline
+    eng.set_guard(None, 0.0)
+    nt = (W + K) * A
+    d_lpr = torch.empty(nt, dtype=torch.float64, device="cuda")
+    eng.chain_device(d_bits, d_lpr)
+    torch.cuda.synchronize()
+    lp64_raw = d_lpr.cpu().numpy()
+    R = min(nt, 32)
+    e0.record(stream)
+    eng.chain_device(d_bits[:R], d_lpr[:R])
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_per_string = e0.elapsed_time(e1) / R
+
+    # roofline of the dominant kernels (the chain-mode passes: fused groups k_group and single steps).  achieved =
+    # the bytes the executed passes must read and write (fused groups keep intermediate tables in shared memory)
+    # over the step-timed time per string; the per-pass event sum and the unfused per-step byte model are reported
+    # beside it
     tot_bytes, per = workloads.pass_bytes(steps, 8, "chain")
     glen, gent = eng.fusion_groups()
     wsum = np.zeros(ns)
@@ -337,15 +399,13 @@ def run_gsb(args):
     wmean = wsum / nprof
     pass_bytes = float(np.sum(gent)) * 8
     kernel_ms = float(wmean.sum())
-    achieved = pass_bytes / (kernel_ms / 1000.0) / 1e9
+    achieved = pass_bytes / (ms_per_string / 1000.0) / 1e9
     fused = [k for k in range(ns) if glen[k] >= 2]
     fused_bytes = float(sum(gent[k] for k in fused)) * 8
     fused_ms = float(sum(wmean[k] for k in fused))
     # DRAM bytes per algorithmic byte of the dominant pass, from one ncu capture of k_group<float2, float, 2, 0> on the
-    # width-27 instance (2.0880 GB read + written for 2.1475 GB algorithmic: no re-reads; writes still dirty in L2
-    # at kernel end make it < 1), scaled to the chain passes of one string
+    # width-27 instance (no re-reads; writes still dirty in L2 at kernel end make it < 1), scaled to one string
     traffic = pass_bytes * K_GROUP_TRAFFIC_RATIO
-    # exact-sample passes (a norm pass where a pass has no other source for its first bit, then the pass)
     sw, sn = eng.profile_steps(strings[0], mode=1)
     sample_kernel_ms = float(sw.sum() + sn.sum())
     _, sent = eng.sample_groups()
@@ -356,75 +416,106 @@ def run_gsb(args):
                                                       "algorithmic byte, times the pass bytes of one string",
                 "peak_kind": peak_kind,
                 "kernel": "chain passes: k_group<float2,float,*> (fused) + k_pair64/k_step (single steps)",
-                "pass_bytes_per_string": pass_bytes, "kernel_ms_per_string": kernel_ms,
+                "pass_bytes_per_string": pass_bytes,
+                "step_timed_ms_per_string": ms_per_string,
+                "step_timed": f"{R} strings in one unguarded chain_device call, CUDA events",
+                "kernel_ms_per_string_event_sum": kernel_ms,
                 "fused_passes_frac": (fused_bytes / (fused_ms / 1000.0) / 1e9) / hbm_peak if fused_ms > 0 else None,
-                "unfused_model_bytes_per_string": float(sum(p[0] for p in per)),
-                "unfused_model_GBps": float(sum(p[0] for p in per)) / (kernel_ms / 1000.0) / 1e9,
+                "model_unfused_bytes_per_string": float(sum(p[0] for p in per)),
+                "model_unfused_GBps": float(sum(p[0] for p in per)) / (ms_per_string / 1000.0) / 1e9,
+                "model_note": "the unfused per-step byte model E*sum(2^r_k + 2^r_k+1); the fused passes move fewer "
+                              "bytes, so this model's GB/s exceeds the copy peak",
                 "passes_per_string": int(sum(1 for x in glen if x > 0)), "fusion": args.fusion,
                 "sample_kernel_ms": sample_kernel_ms, "sample_norm_ms": float(sn.sum()),
-                "sample_write_ms": float(sw.sum()), "sample_unfused_model_bytes": sample_bytes,
+                "sample_write_ms": float(sw.sum()), "model_unfused_sample_bytes": sample_bytes,
                 "sample_pass_bytes": sample_pass_bytes,
                 "sample_achieved": sample_pass_bytes / (sample_kernel_ms / 1000.0) / 1e9,
                 "sample_frac": sample_pass_bytes / (sample_kernel_ms / 1000.0) / 1e9 / hbm_peak}
-    eng.close()
 
-    # complex128 plain form on the first strings of the timed batch, and the c64-vs-c128 agreement
+    # complex128 plain form: amplitudes/s, every timed string and every sample again, s/sample
     c128 = {}
-    if args.c128_amps > 0:
-        e128 = gsb.Engine.from_text(w["plan"], precision=128, device=local)
-        e128.set_fusion(args.fusion)
-        tune128 = e128.autotune(mode=2, reps=3) if args.autotune else None
-        e128.set_stream(stream.cuda_stream)
-        B = args.c128_amps
-        d_lp128 = torch.empty(B, dtype=torch.float64, device="cuda")
-        d_cond128 = torch.empty((B, ns), dtype=torch.float64, device="cuda")
+    if args.c128:
+        B = min(args.c128_amps, K * A)
+        d_lp128 = torch.empty(nt, dtype=torch.float64, device="cuda")
+        d_cond128 = torch.empty((nt, ns), dtype=torch.float64, device="cuda")
         sl = slice(W * A, W * A + B)
         e128.chain_device(d_bits[:1], d_lp128[:1], d_cond128[:1])
         torch.cuda.synchronize()
         e0.record(stream)
-        e128.chain_device(d_bits[sl], d_lp128, d_cond128)
+        e128.chain_device(d_bits[sl], d_lp128[sl], d_cond128[sl])
         e1.record(stream)
         torch.cuda.synchronize()
         amps128 = B / (e0.elapsed_time(e1) / 1000.0)
+        e128.chain_device(d_bits, d_lp128, d_cond128)
+        torch.cuda.synchronize()
         lp128 = d_lp128.cpu().numpy()
-        dlp = float(np.abs(lp128 - lp64[sl]).max())
-        dcond = float(np.abs(d_cond128.cpu().numpy() - cond64[sl]).max())
-        S2 = args.c128_samples
+        dlp = np.abs(lp128 - lp64)
+        dlp_raw = np.abs(lp128 - lp64_raw)
+        d_sb128 = torch.empty((S, ns), dtype=torch.int8, device="cuda")
+        d_slp128 = torch.empty(S, dtype=torch.float64, device="cuda")
 
         def time_samples128():
-            e128.sample_device(d_u[:1], d_sb[:1], d_slp[:1])      # graph built outside the timed region
+            e128.sample_device(d_u[:1], d_sb128[:1], d_slp128[:1])   # graph built outside the timed region
             torch.cuda.synchronize()
             e0.record(stream)
-            e128.sample_device(d_u[:S2], d_sb[:S2], d_slp[:S2])
+            e128.sample_device(d_u, d_sb128, d_slp128)
             e1.record(stream)
             torch.cuda.synchronize()
-            return e0.elapsed_time(e1) / 1000.0 / S2
+            return e0.elapsed_time(e1) / 1000.0 / S
 
         s_per_sample128 = time_samples128()
-        same_bits = bool((d_sb[:S2].cpu().numpy() == sbits64[:S2]).all())
+        same_bits = bool((d_sb128.cpu().numpy() == sbits64).all())
+        dslp = np.abs(d_slp128.cpu().numpy() - slp64)
         # the same complex128 form without fusion: one norm pass and one write pass per DP step, the structure of
         # the reference executor's two-pass sampler (gsamp2.cpp:39-55)
         e128.set_fusion(1)
         s_per_sample128_unfused = time_samples128()
-        e128.close()
+        x = lp128 + ns
         c128 = {"amps_per_s": amps128, "autotune_ms_item_before_after": tune128,
                 "s_per_sample": s_per_sample128, "s_per_sample_unfused_two_pass": s_per_sample128_unfused,
-                "max_abs_dlog2p_c64_vs_c128": dlp,
-                "max_abs_dcond_c64_vs_c128": dcond, "samples_same_bits_c64_c128": same_bits}
+                "samples_per_s_ratio_c64_over_c128": s_per_sample128 / s_per_sample64,
+                "check": {"strings": int(nt), "samples": int(S), "tol": args.tol,
+                          "max_abs_dlog2p_c64_vs_c128": float(dlp.max()),
+                          "strings_above_tol": int((dlp > args.tol).sum()),
+                          "max_abs_dlog2p_c64_unguarded": float(dlp_raw.max()),
+                          "unguarded_above_tol": int((dlp_raw > args.tol).sum()),
+                          "median_abs_dlog2p_times_sqrt_x_unguarded": float(np.median(dlp_raw * np.sqrt(2.0 ** x))),
+                          "samples_max_abs_dlog2p": float(dslp.max()), "samples_same_bits_c64_c128": same_bits}}
+    eng.close()
+    e128.close()
 
-    # per string: begin + one launch per chain pass + finish; one item reset per batch
-    launches = (roofline["passes_per_string"] + 2) * K * A + K
+    guard = {"enabled": bool(args.guard), "log2_xmin": lx, "tol": args.tol,
+             "strings_reevaluated_in_timed_region": int(guarded_timed),
+             "fraction_of_timed_strings": guarded_timed / float(K * A),
+             "model": "|d log2 Pr| ~ N(0, (s1 sqrt(ns) / sqrt(x))^2), x = Pr 2^ns; re-evaluated where "
+                      "z s1 sqrt(ns) / sqrt(x) > tol"}
+    # per string: begin + one launch per chain pass + finish; one item reset per batch; guard re-evaluations
+    launches = (roofline["passes_per_string"] + 2) * K * A + K + guarded_timed * (roofline["passes_per_string"] + 2)
     out = {
         "metric": METRIC, "value": value, "unit": "amps/s", "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": f"c64 arena, f{args.arith} arithmetic", "data": "synthetic",
+        "dtype": f"c64 arena, f{args.arith} arithmetic" + (", c128 guard" if args.guard else ""), "data": "synthetic",
         "config": {"workload": WORKLOAD, "n": 70, "width": w["width"], "strings_per_step": A, "mode": "chain",
-                   "arith": args.arith, "fusion": args.fusion, "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
+                   "arith": args.arith, "fusion": args.fusion, "guard": bool(args.guard),
+                   "parallelism": f"replicas{world}", "l2": "inputs larger than L2: arena 8.6 GB >> 126 MB"},
         "s_per_sample": s_per_sample64, "samples_per_s": world / s_per_sample64,
-        "c128": c128, "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
+        "c128": c128, "guard": guard, "e2e": e2e, "roofline": roofline, "gpu_launches": launches,
         "autotune_ms_item_before_after": tune64,
         "clocks": clk.summary(),
     }
+    if rank == 0 and world == 1 and args.ref_gpu_port:
+        try:
+            with tempfile.TemporaryDirectory() as td:
+                plan = os.path.join(td, "plan.txt")
+                open(plan, "w").write(w["plan"])
+                rg = ref_gpu_port_time(plan, strings[W * A:W * A + 4], ns)
+            if rg:
+                rg["max_abs_dlog2p_vs_c128"] = float(np.abs(np.array(rg.pop("log2p")) - lp128[W * A:W * A + 4]).max()) \
+                    if c128 else None
+                rg["value_over_port"] = value / rg["amps_per_s"]
+                out["reference_gpu_port"] = rg
+        except Exception as ex:   # the port is a reported comparison only
+            out["reference_gpu_port"] = {"unavailable": str(ex)[:200]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         with tempfile.TemporaryDirectory() as td:
             plan = os.path.join(td, "plan.txt")
@@ -434,9 +525,11 @@ def run_gsb(args):
             cores = os.cpu_count() or 1
             t, txt, kind = ref_time(plan, ["chain", sp], cores)
             ref_lp = float(txt.split()[0])
+            from oracle import ref_isa
             out["cpu_baseline"] = {"value": 1.0 / t, "unit": "amps/s", "cores": cores, "kind": kind,
-                                   "sample": "1 uniform random string of the workload, gsamp2 chain mode (complex64)",
-                                   "abs_dlog2p_vs_gpu_c64": abs(ref_lp - float(lp64[W * A]))}
+                                   "sample": "1 uniform random string of the workload, gsamp2 chain mode (complex64"
+                                             + (f", -march=x86-64-{ref_isa(64)}" if kind == "reference" else "") + ")",
+                                   "abs_dlog2p_vs_gpu_c128": abs(ref_lp - float(lp128[W * A])) if c128 else None}
     if rank == 0:
         print(json.dumps(out), flush=True)
     replicas.finish(world)
@@ -455,7 +548,7 @@ def run_form_batch(args):
     import gsb
     import workloads
     t0 = time.perf_counter()
-    bw = workloads.batch_workload(count=args.batch_instances, seed=0, npre=16, nsuf=4)
+    bw = workloads.batch_workload(count=args.batch_instances, seed=0, npre=16, nsuf=4, order=args.batch_order)
     t_plan = time.perf_counter() - t0
     plans = [w["plan"] for w in bw["instances"]]
     widths = [w["width"] for w in bw["instances"]]
@@ -498,13 +591,15 @@ def run_form_batch(args):
                                                                                  "ctas_per_sm": per_sm},
                    "c128": {"ms_per_launch": ms128, "max_abs_dlog2p_c64_vs_c128": float(d.max()),
                             "median_abs_dlog2p": float(np.median(d))},
-                   "roofline": {"bound": "hbm", "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                                "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
-                                "note": "team tables <= 2^20 entries: many items are L2-resident"},
-                   "roofline_l2": {"bound": "l2", "achieved": byt / (ms / 1e3) / 1e9, "peak": l2, "unit": "GB/s",
-                                   "frac": byt / (ms / 1e3) / 1e9 / l2,
-                                   "peak_kind": "measured here: L2 copy bandwidth (gsb_probe_l2_copy, best of "
-                                                "16/24/32 MiB buffers, one launch of 400 passes)"},
+                   "roofline": {"bound": "l2", "achieved": byt / (ms / 1e3) / 1e9, "peak": l2, "unit": "GB/s",
+                                "frac": byt / (ms / 1e3) / 1e9 / l2,
+                                "peak_kind": "measured here: L2 copy bandwidth (gsb_probe_l2_copy, best of "
+                                             "16/24/32 MiB buffers, one launch of 400 passes)",
+                                "note": "team tables of <= 2^20 entries, each reused through an item's prefix and "
+                                        "suffix sweeps: the launch reads and writes them mostly in L2"},
+                   "roofline_hbm": {"bound": "hbm", "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                                    "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_kind": kind},
+                   "orders": args.batch_order,
                    "host_planning_s": t_plan, "steps": args.steps, "warmup": args.warmup,
                })
 
@@ -576,25 +671,31 @@ def run_form_wide34(args):
         t_smp = time.perf_counter() - t2
         chain_bytes = 8.0 * float(eng.fusion_groups()[1].sum())     # bytes the executed passes move per string
         sample_bytes = 8.0 * float(eng.sample_groups()[1].sum())
-    # complex128 cross-check of 4 amplitudes: a second order with 3 slice vertices cut out (width 33), every slice's
-    # final table from 'prefix', summed by 'resume' (the reference's slicing identity)
+    # complex128 cross-check of 4 amplitudes: a second order with 10 slice vertices cut out (width 30), every
+    # slice's final table from 'prefix' through the last step, summed by 'resume' (the reference's slicing identity,
+    # gsamp2.cpp:176-208); one complex128 arena serves all 1,024 slice plans (they differ only in M)
     t3 = time.perf_counter()
     sl = workloads.wide34_slices(w)
     v1 = [s["v"] for s in w["steps"]]
+    lines = []
+    for i in range(4):
+        q = np.zeros(w["n"], np.int8)
+        q[v1] = strings[i]
+        lines.append(q[sl["step_vertices"]])
+    dumps = [[] for _ in lines]
+    lss = [[] for _ in lines]
     check = []
     with gsb.Engine.from_text(sl["plans"][0], precision=gsb.GSB_C128) as e128:
         ns2 = e128.ns
-        for i in range(4):
-            q = np.zeros(w["n"], np.int8)
-            q[v1] = strings[i]
-            line = q[sl["step_vertices"]]
-            dumps, lss = [], []
-            for text in sl["plans"]:
-                e128.set_matrices_from_text(text)
+        for text in sl["plans"]:
+            e128.set_matrices_from_text(text)
+            for i, line in enumerate(lines):
                 d, ls, _ = e128.prefix(line, ns2)
-                dumps.append(d)
-                lss.append(ls)
-            _, lpf, _, _ = e128.resume(line, ns2, 0, 0, dumps, lss)
+                dumps[i].append(d)
+                lss[i].append(ls)
+        e128.set_matrices_from_text(sl["plans"][0])
+        for i, line in enumerate(lines):
+            _, lpf, _, _ = e128.resume(line, ns2, 0, 0, dumps[i], lss[i])
             check.append((float(lp[i]), float(lpf)))
     t_check = time.perf_counter() - t3
     _form_line("wide34", "amps/s and s/sample at n=80, width 34, complex64 (137 GB arena)", 256 / t_amp, "amps/s", True, {
@@ -613,8 +714,51 @@ def run_form_wide34(args):
                               "max_abs_dlog2p": max(abs(a - b) for a, b in check), "seconds": t_check}})
 
 
+def run_form_hybrid(args):
+    """Hybrid rejection sampling of the headline instance in process (hybrid_sampler, the reference's doped_sampler
+    driver with the executor kept loaded): proposals draw the first 70 - m step bits uniformly and sample the last
+    m = 16 exactly.  Seconds per proposal with the proposals batched into gsb_hybrid calls, and with one call per
+    proposal (the reference's structure without its process start-up)."""
+    import gsb
+    import hybrid_sampler
+    import workloads
+    w = workloads.matching_n70_w30()
+    with tempfile.TemporaryDirectory() as td:
+        plan = os.path.join(td, "plan.txt")
+        open(plan, "w").write(w["plan"])
+        sv = os.path.join(td, "sv.json")
+        json.dump([s["v"] for s in w["steps"]], open(sv, "w"))
+        hs = hybrid_sampler.HybridSampler(plan, sv, na=0, nd=70, m=16, precision=64)
+        hs.sample(4, 1, 2.0, os.path.join(td, "warm.txt"))
+        res = {}
+        for name, batch in (("batched", 64), ("one_call_per_proposal", 1)):
+            hs.BATCH = batch
+            gsb.Engine.synchronize(hs.eng)
+            t0 = time.perf_counter()
+            acc, zmax = hs.sample(args.proposals, 7, 2.0, os.path.join(td, f"{name}.txt"))
+            gsb.Engine.synchronize(hs.eng)
+            res[name] = (time.perf_counter() - t0) / args.proposals
+        same = open(os.path.join(td, "batched.txt")).read().split("\n")
+        one = open(os.path.join(td, "one_call_per_proposal.txt")).read().split("\n")
+        import re
+
+        def strip(ls):   # the lines without their wall-time fields
+            return [" ".join(t for t in ln.split() if not re.fullmatch(r"[0-9.]+s", t)) for ln in ls]
+        hs.close()
+    _form_line("hybrid", "s/proposal (hybrid rejection sampling, n=70 w=30, m=16, complex64)", res["batched"],
+               "s/proposal", False,
+               {"config": {"workload": WORKLOAD, "proposals": args.proposals, "m_suffix": 16, "cap": 2.0},
+                "one_call_per_proposal_s": res["one_call_per_proposal"],
+                "batched_over_single": res["one_call_per_proposal"] / res["batched"],
+                "same_decisions_and_bits": strip(same) == strip(one),
+                "accepted": acc, "max_z": zmax})
+
+
 if __name__ == "__main__":
     a = parse()
+    if a.form == "hybrid":
+        run_form_hybrid(a)
+        raise SystemExit(0)
     if a.form == "batch":
         run_form_batch(a)
     elif a.form == "grad":

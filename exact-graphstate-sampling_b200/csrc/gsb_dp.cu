@@ -371,21 +371,24 @@ int gsb_dp_extend(int r, int rn, uint64_t rho, uint64_t pivmask, int nker, const
         int p;
         ~Restore() { cudaSetDevice(p); }
     } restore{prev};
-    double2 *a = nullptr, *b = nullptr;
-    double *w = nullptr;
+    struct Buffers {   // freed on every return path (cudaFree of a null pointer does nothing)
+        double2 *a = nullptr, *b = nullptr;
+        double *w = nullptr;
+        ~Buffers() {
+            cudaFree(a);
+            cudaFree(b);
+            cudaFree(w);
+        }
+    } m;
     const size_t na = (size_t)1 << r, nb = (size_t)1 << rn;
-    DP_CK(cudaMalloc(&a, na * 16));
-    DP_CK(cudaMalloc(&b, nb * 16));
-    DP_CK(cudaMalloc(&w, 32));
-    DP_CK(cudaMemcpy(a, old, na * 16, cudaMemcpyHostToDevice));
-    DP_CK(cudaMemcpy(w, wv, 32, cudaMemcpyHostToDevice));
-    k_dp_step<double2><<<dp_grid(rn, 4096), 256>>>(st, a, b, w);
-    cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaMemcpy(out, b, nb * 16, cudaMemcpyDeviceToHost);
-    cudaFree(a);
-    cudaFree(b);
-    cudaFree(w);
-    DP_CK(e);
+    DP_CK(cudaMalloc(&m.a, na * 16));
+    DP_CK(cudaMalloc(&m.b, nb * 16));
+    DP_CK(cudaMalloc(&m.w, 32));
+    DP_CK(cudaMemcpy(m.a, old, na * 16, cudaMemcpyHostToDevice));
+    DP_CK(cudaMemcpy(m.w, wv, 32, cudaMemcpyHostToDevice));
+    k_dp_step<double2><<<dp_grid(rn, 4096), 256>>>(st, m.a, m.b, m.w);
+    DP_CK(cudaGetLastError());
+    DP_CK(cudaMemcpy(out, m.b, nb * 16, cudaMemcpyDeviceToHost));
     return 0;
 }
 

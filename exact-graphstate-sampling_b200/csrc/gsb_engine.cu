@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -171,8 +172,15 @@ struct Engine {
     std::vector<Launch> lw, ln;
     std::map<int, cudaGraphExec_t> graphs;   // key: graph kind
     std::map<void *, int> occ;
+    // complex128 re-evaluation of unlikely strings (gsb_set_guard): the engine that re-evaluates this one's strings
+    // whose log2 Pr + ns < guard_lx, and the engine this one re-evaluates for
+    Engine *guard = nullptr, *guarded = nullptr;
+    double guard_lx = 0;
+    int64_t guard_evals = 0;
 
     ~Engine() {
+        if (guard) guard->guarded = nullptr;
+        if (guarded) guarded->guard = nullptr;
         DevGuard g(dev);
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
         cudaFree(mem);
@@ -479,6 +487,21 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
             for (int x = 0; x < 2; x++) { a.Mr[b][x] = hs.Mr[b][x]; a.Mi[b][x] = hs.Mi[b][x]; }
             a.c[b] = hs.Mr[b][0] * hs.Mr[b][0] + hs.Mi[b][0] * hs.Mi[b][0] + hs.Mr[b][1] * hs.Mr[b][1] +
                      hs.Mi[b][1] * hs.Mi[b][1];
+            // factored form of a written complex64 step: pivot on the larger coefficient of the row
+            const double n0 = hs.Mr[b][0] * hs.Mr[b][0] + hs.Mi[b][0] * hs.Mi[b][0];
+            const double n1 = hs.Mr[b][1] * hs.Mr[b][1] + hs.Mi[b][1] * hs.Mi[b][1];
+            a.piv[b] = -1;
+            a.br[b] = a.bi[b] = 0;
+            a.cp[b] = 1;
+            if (E.prec == 64 && kinds[s] != GK_ANY && std::max(n0, n1) > 0) {
+                const int pv = n0 >= n1 ? 0 : 1;
+                const std::complex<double> w(hs.Mr[b][pv], hs.Mi[b][pv]), o(hs.Mr[b][1 - pv], hs.Mi[b][1 - pv]);
+                const std::complex<double> beta = o / w;
+                a.piv[b] = pv;
+                a.br[b] = beta.real();
+                a.bi[b] = beta.imag();
+                a.cp[b] = std::norm(w);
+            }
         }
         for (int j = 0; j < g.nmem; j++) {
             for (int t = 0; t < g.ntq; t++) a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
@@ -807,6 +830,91 @@ static int forced_batch(Engine *E, int kind, const int8_t *bits, int64_t nstr, d
     return 0;
 }
 
+// ---- complex128 guard (gsb_set_guard) ----
+// A complex64 log2 Pr carries a rounding error that grows as 1 / sqrt(Pr 2^ns) (the table's rounding is absolute
+// in units of its norm, and an unlikely string's amplitude is a small remainder of it); strings below the guard's
+// threshold are evaluated again by the complex128 engine, whose results replace the complex64 ones.
+static void guard_pick(const Engine *E, const double *lp, int64_t n, std::vector<int64_t> &idx) {
+    const double ns = E->plan.ns;
+    for (int64_t i = 0; i < n; i++)
+        if (!(lp[i] + ns >= E->guard_lx)) idx.push_back(i);   // -inf and NaN too
+}
+
+// host arrays: kind 0 (chain: log2 Pr and conditionals) or 1 (prob: log2 Pr)
+static int guard_host(Engine *E, int kind, const int8_t *bits, int64_t nstr, double *log2p, double *cond) {
+    if (!E->guard || nstr <= 0) return 0;
+    std::vector<int64_t> idx;
+    guard_pick(E, log2p, nstr, idx);
+    if (idx.empty()) return 0;
+    const int ns = E->plan.ns;
+    const size_t m = idx.size(), nsz = (size_t)std::max(ns, 1);
+    std::vector<int8_t> b(m * nsz);
+    std::vector<double> lp(m), cd(cond ? m * nsz : 0);
+    for (size_t j = 0; j < m; j++) memcpy(b.data() + j * nsz, bits + idx[j] * ns, (size_t)ns);
+    Engine *G = E->guard;
+    {
+        DevGuard g(G->dev);
+        int rc = forced_batch(G, kind, b.data(), (int64_t)m, lp.data(), cond ? cd.data() : nullptr);
+        if (rc) return rc;
+    }
+    for (size_t j = 0; j < m; j++) {
+        log2p[idx[j]] = lp[j];
+        if (cond) memcpy(cond + idx[j] * ns, cd.data() + j * nsz, (size_t)ns * 8);
+    }
+    E->guard_evals += (int64_t)m;
+    return 0;
+}
+
+// device arrays (the engines share a device): the strings' rows are copied to the guard, its results copied back
+static int guard_device(Engine *E, int kind, const int8_t *d_bits, int64_t nstr, double *d_log2p, double *d_cond) {
+    if (!E->guard || nstr <= 0) return 0;
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    std::vector<double> lp((size_t)nstr);
+    GSB_CK(cudaMemcpy(lp.data(), d_log2p, (size_t)nstr * 8, cudaMemcpyDeviceToHost));
+    std::vector<int64_t> idx;
+    guard_pick(E, lp.data(), nstr, idx);
+    if (idx.empty()) return 0;
+    Engine *G = E->guard;
+    DevGuard g(G->dev);
+    const int ns = E->plan.ns;
+    for (size_t off = 0; off < idx.size(); off += (size_t)G->cap) {
+        const size_t m = std::min(idx.size() - off, (size_t)G->cap);
+        for (size_t j = 0; j < m && ns; j++)
+            GSB_CK(cudaMemcpyAsync(G->d_forced + j * ns, d_bits + idx[off + j] * ns, (size_t)ns, cudaMemcpyDeviceToDevice,
+                                   G->stream));
+        int rc = G->run_graph_items(kind, (int64_t)m);
+        if (rc) return rc;
+        for (size_t j = 0; j < m; j++) {
+            GSB_CK(cudaMemcpyAsync(d_log2p + idx[off + j], G->d_logp + j, 8, cudaMemcpyDeviceToDevice, G->stream));
+            if (d_cond && ns)
+                GSB_CK(cudaMemcpyAsync(d_cond + idx[off + j] * ns, G->d_cond + j * ns, (size_t)ns * 8,
+                                       cudaMemcpyDeviceToDevice, G->stream));
+        }
+    }
+    GSB_CK(cudaStreamSynchronize(G->stream));
+    int rc = check_device(G);
+    if (rc) return rc;
+    E->guard_evals += (int64_t)idx.size();
+    return 0;
+}
+
+static bool same_plan(const HPlan &a, const HPlan &b) {
+    if (a.n != b.n || a.ns != b.ns || a.R != b.R || a.st.size() != b.st.size()) return false;
+    for (size_t k = 0; k < a.st.size(); k++) {
+        const HStep &x = a.st[k], &y = b.st[k];
+        if (x.v != y.v || x.nk != y.nk || x.m != y.m || x.g != y.g || x.rhoc != y.rhoc || x.tk != y.tk ||
+            x.t.size() != y.t.size())
+            return false;
+        for (size_t i = 0; i < x.t.size(); i++)
+            if (x.t[i].tq != y.t[i].tq || x.t[i].x != y.t[i].x || x.t[i].tau != y.t[i].tau || x.t[i].par != y.t[i].par)
+                return false;
+        for (int r = 0; r < 2; r++)
+            for (int c = 0; c < 2; c++)
+                if (x.Mr[r][c] != y.Mr[r][c] || x.Mi[r][c] != y.Mi[r][c]) return false;
+    }
+    return true;
+}
+
 int gsb_prob(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p) {
     if (!e) return fail(GSB_E_STATE, "null engine");
     if (nstr < 0 || (nstr && (!bits || !log2p))) return fail(GSB_E_USAGE, "null argument");
@@ -814,7 +922,8 @@ int gsb_prob(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p) {
     DevGuard g(E->dev);
     int rc = check_bits(bits, nstr, E->plan.ns, false);
     if (rc) return rc;
-    return forced_batch(E, 1, bits, nstr, log2p, nullptr);
+    if ((rc = forced_batch(E, 1, bits, nstr, log2p, nullptr))) return rc;
+    return guard_host(E, 1, bits, nstr, log2p, nullptr);
 }
 
 int gsb_chain(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p, double *cond) {
@@ -824,7 +933,8 @@ int gsb_chain(gsb_engine *e, const int8_t *bits, int64_t nstr, double *log2p, do
     DevGuard g(E->dev);
     int rc = check_bits(bits, nstr, E->plan.ns, false);
     if (rc) return rc;
-    return forced_batch(E, 0, bits, nstr, log2p, cond);
+    if ((rc = forced_batch(E, 0, bits, nstr, log2p, cond))) return rc;
+    return guard_host(E, 0, bits, nstr, log2p, cond);
 }
 
 static int uniform_batch(Engine *E, const double *u, int64_t count, int8_t *bits, double *log2p) {
@@ -838,6 +948,8 @@ static int uniform_batch(Engine *E, const double *u, int64_t count, int8_t *bits
         if (bits && ns) GSB_CK(cudaMemcpyAsync(bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToHost, E->stream));
         GSB_CK(cudaStreamSynchronize(E->stream));
         if ((rc = check_device(E))) return rc;
+        // guarded: the log2 Pr of an unlikely sample again in complex128 (its bits are the complex64 draw's)
+        if (bits && log2p && (rc = guard_host(E, 0, bits + off * ns, nb, log2p + off, nullptr))) return rc;
     }
     return 0;
 }
@@ -1084,7 +1196,7 @@ int gsb_chain_device(gsb_engine *e, const int8_t *d_bits, int64_t nstr, double *
         GSB_CK(cudaMemcpyAsync(d_log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToDevice, E->stream));
         if (d_cond && ns) GSB_CK(cudaMemcpyAsync(d_cond + off * ns, E->d_cond, (size_t)(nb * ns) * 8, cudaMemcpyDeviceToDevice, E->stream));
     }
-    return 0;
+    return guard_device(E, 0, d_bits, nstr, d_log2p, d_cond);
 }
 
 int gsb_sample_device(gsb_engine *e, const double *d_u, int64_t count, int8_t *d_bits, double *d_log2p) {
@@ -1101,7 +1213,7 @@ int gsb_sample_device(gsb_engine *e, const double *d_u, int64_t count, int8_t *d
         GSB_CK(cudaMemcpyAsync(d_log2p + off, E->d_logp, (size_t)nb * 8, cudaMemcpyDeviceToDevice, E->stream));
         if (ns) GSB_CK(cudaMemcpyAsync(d_bits + off * ns, E->d_bits, (size_t)(nb * ns), cudaMemcpyDeviceToDevice, E->stream));
     }
-    return 0;
+    return guard_device(E, 0, d_bits, count, d_log2p, nullptr);
 }
 
 int gsb_synchronize(gsb_engine *e) {
@@ -1110,6 +1222,34 @@ int gsb_synchronize(gsb_engine *e) {
     DevGuard g(E->dev);
     GSB_CK(cudaStreamSynchronize(E->stream));
     return check_device(E);
+}
+
+int gsb_set_guard(gsb_engine *e, gsb_engine *g, double log2_xmin) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    if (E->prec != 64) return fail(GSB_E_USAGE, "the guarded engine must be complex64");
+    if (E->guard) {
+        E->guard->guarded = nullptr;
+        E->guard = nullptr;
+    }
+    E->guard_evals = 0;
+    if (!g) return 0;
+    Engine *G = eng(g);
+    if (G->prec != 128) return fail(GSB_E_USAGE, "the guard engine must be complex128");
+    if (G->dev != E->dev) return fail(GSB_E_USAGE, "the guard engine must be on the same device");
+    if (G->guarded && G->guarded != E) return fail(GSB_E_USAGE, "the guard engine already guards another engine");
+    if (!same_plan(E->plan, G->plan)) return fail(GSB_E_USAGE, "the guard engine's plan differs");
+    if (!(log2_xmin == log2_xmin)) return fail(GSB_E_USAGE, "threshold is NaN");
+    E->guard = G;
+    G->guarded = E;
+    E->guard_lx = log2_xmin;
+    return 0;
+}
+
+int gsb_guard_evaluations(const gsb_engine *e, int64_t *count) {
+    if (!e || !count) return fail(GSB_E_USAGE, "null argument");
+    *count = eng(e)->guard_evals;
+    return 0;
 }
 
 int gsb_set_arith(gsb_engine *e, int bits) {
@@ -1385,7 +1525,8 @@ int gsb_test_withhold_tile_loads(gsb_engine *e, int on) {
     Engine *E = eng(e);
     DevGuard g(E->dev);
     GSB_CK(cudaStreamSynchronize(E->stream));
-    E->withhold_loads = on ? 1 : 0;
+    if (on < 0 || on > 2) return fail(GSB_E_USAGE, "withhold mode must be 0, 1 or 2");
+    E->withhold_loads = on;
     for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);   // the graphs hold the pass arguments by value
     E->graphs.clear();
     return 0;

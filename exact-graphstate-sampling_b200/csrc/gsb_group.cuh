@@ -23,11 +23,18 @@ struct GroupStepArgs {
     int tau0[4], tau1[4], par[4];
     uint64_t lambda;
     double Mr[2][2], Mi[2][2];
+    // factored written step (complex64 arena), per bit b: pivot column (-1: not factored), beta = M[b][1-piv] /
+    // M[b][piv] and cp = |M[b][piv]|^2 (1 when not factored): the stored table is the true one divided by M[b][piv]
+    int piv[2];
+    double br[2], bi[2], cp[2];
     unsigned char in_idx[16][4], out_idx[16][2], mpar[16];
 };
 
 // first-bit source of a sampling pass (group_decide)
 enum { GSRC_ANALYTIC = 0, GSRC_TRAILING = 1, GSRC_NORM = 2 };
+// absolute accuracy assumed of a branch probability estimated from a trailing step's shared sums (FP32 sums of
+// order A + B, rounded at 2^-24, over up to 2^30 entries in per-thread and per-tile partials)
+constexpr double TRX_FLOOR = 1.0 / (1 << 20);
 
 struct GroupArgs {
     int d, L, nbhi, ssz[4];
@@ -80,6 +87,11 @@ __device__ __forceinline__ bool grid_reduceN(double (&a)[ND], const Ctx &cx, dou
     __syncthreads();
     if (!last) return false;
     __threadfence();
+    if (*(volatile int *)&cx.st->err) {
+        // a block of this launch gave up waiting (it counted itself and left): no totals, no epilogue
+        if (threadIdx.x == 0) cx.st->counter = 0;
+        return false;
+    }
     double s[ND];
 #pragma unroll
     for (int i = 0; i < ND; i++) s[i] = 0;
@@ -104,13 +116,16 @@ __device__ __forceinline__ bool grid_reduceN(double (&a)[ND], const Ctx &cx, dou
 }
 
 // Scalar logic after a fused chain1 pass: the conditionals of every step of the group (gsamp2.cpp:59-70).
+// cp[s]: |M[b_s][piv]|^2 of a factored step (its stored norm is the true one over cp), 1 otherwise.
 template <int D>
-__device__ __forceinline__ void group_chain1_epilogue(const Ctx &cx, int k0, const double (&nb)[D]) {
+__device__ __forceinline__ void group_chain1_epilogue(const Ctx &cx, int k0, const double (&nb)[D], const double (&cp)[D]) {
     DevState *st = cx.st;
     const size_t row = (size_t)st->item * (size_t)cx.ns;
     double prev = st->prev;
+    double lcp = 0;
     for (int s = 0; s < D; s++) {
-        const double c = s == 0 ? ldexp(nb[0], 2 * st->ek) / (2 * prev) : nb[s] / (2 * nb[s - 1]);
+        const double c = (s == 0 ? ldexp(nb[0], 2 * st->ek) / (2 * prev) : nb[s] / (2 * nb[s - 1])) * cp[s];
+        lcp += log2(cp[s]);
         cx.cond_out[row + k0 + s] = c;
         if (!(nb[s] > 0)) {
             for (int j = k0 + s; j < cx.ns; j++) cx.cond_out[row + j] = 0;
@@ -121,7 +136,7 @@ __device__ __forceinline__ void group_chain1_epilogue(const Ctx &cx, int k0, con
         }
         prev = nb[s];
     }
-    st->lsc += st->ek;
+    st->lsc += st->ek + 0.5 * lcp;
     st->prev = nb[D - 1];
     int ex;
     frexp(nb[D - 1], &ex);
@@ -542,6 +557,285 @@ __device__ __forceinline__ void group_cosets_pk(const GroupArgs &ga, const Group
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Factored written steps (complex64 arena).  A written step stores out = M[b][0] S0 + s_c M[b][1] S1 per output
+// (S0 / S1: the output's x = 0 / signed x = 1 sums).  With the pivot w = M[b][PIV], the larger of the two
+// coefficients, the step stores out / w instead:
+//   PIV = 0:  P + beta s_c Q,  P = sc S0,             Q = S1, beta = sc M[b][1] / M[b][0]
+//   PIV = 1:  P + beta Q,      P = sc s_c S1,         Q = S0, beta = sc M[b][0] / M[b][1]
+// so every output costs one complex product (beta Q) instead of two, and a sum starts from its first term instead
+// of from zero.  |beta| <= sc.  The complex factor w of the whole table is left out of the stored values; the
+// normalised samplers depend on ratios of norms only, and the 'chain' epilogue multiplies each step's norm ratio by
+// |w|^2 (GroupStepArgs::cp).  sc is the pass's scale (first step, SC = true) or 1 (later steps of the pass).
+// Shapes are the compile-time GK_* shapes (m = 2): offset t's x = 0 term goes to output o0(t) = (t >= NTQ - H),
+// its x = 1 term to 1 - o0(t).
+template <int NTQ, int H, int PIV>
+struct FShape {
+    // output of offset t's P-side term / Q-side term
+    __host__ __device__ static constexpr int pout(int t) { return (PIV == 0) == (t < NTQ - H) ? 0 : 1; }
+    __host__ __device__ static constexpr int qout(int t) { return 1 - pout(t); }
+    __host__ __device__ static constexpr int first_p(int tau) {
+        for (int t = 0; t < NTQ; t++)
+            if (pout(t) == tau) return t;
+        return -1;
+    }
+    __host__ __device__ static constexpr int first_q(int tau) {
+        for (int t = 0; t < NTQ; t++)
+            if (qout(t) == tau) return t;
+        return -1;
+    }
+};
+
+template <typename E, typename T, int P, int NTQ, int H, int PIV, bool SC, bool FIRST, bool LAST, bool STS>
+__device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
+                                               const uint64_t TB, const int L, const uint32_t in, const uint32_t out,
+                                               const T sc, const T br, const T bi, T &nsum) {
+    typedef typename CplxOf<T>::type V;
+    typedef FShape<NTQ, H, PIV> S;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - (P == 2 ? 1 : 0);
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    T sg[NTQ];
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) sg[t] = gs.par[t] ? (T)-1 : (T)1;
+    // Q sums start from their first term: PIV = 0 folds that term's sign into beta, later terms carry the relative
+    // sign; PIV = 1 sums x = 0 terms, which have none.  P coefficients: sc (PIV = 0), sc * sign of the term (PIV = 1,
+    // times the class sign per class).
+    T qbr[2], qbi[2], rel[NTQ], pcf[NTQ];
+#pragma unroll
+    for (int tau = 0; tau < 2; tau++) {
+        const int f = S::first_q(tau);
+        const T s = (PIV == 0 && f >= 0) ? sg[f < 0 ? 0 : f] : (T)1;
+        qbr[tau] = br * s;
+        qbi[tau] = bi * s;
+    }
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) {
+        const int f = S::first_q(S::qout(t));
+        rel[t] = PIV == 0 ? sg[t] * sg[f < 0 ? 0 : f] : (T)1;
+        pcf[t] = PIV == 0 ? sc : sc * sg[t];
+    }
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t zl[NTQ], ib[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            ib[t] = (uint32_t)gs.in_idx[j][t] * NC;
+            zl[t] = FIRST ? ga.z0lo[j][t] : 0u;
+        }
+        uint32_t ol[2] = {0, 0}, oidx[2] = {0, 0};
+        E *ob[2] = {mem, mem};
+#pragma unroll
+        for (int tau = 0; tau < 2; tau++) {
+            oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
+            ol[tau] = LAST ? ga.zdlo[j][tau] : 0u;
+            if (LAST) ob[tau] = mem + (TB ^ ga.blk_out[gs.out_idx[j][tau]]);
+        }
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = (uint32_t)P * g;
+            bool neg[P];
+#pragma unroll
+            for (int c = 0; c < P; c++) neg[c] = ((mp ^ __popc(pc & lam) ^ __popc((uint32_t)c & lam)) & 1) != 0;
+            T pr[P][2], pi[P][2], qr[P][2], qi[P][2];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                T vr[P], vi[P];
+                if (FIRST) ld_perm<P>(reinterpret_cast<const E *>(smem + in) + ib[t], pc ^ zl[t], vr, vi);
+                else lds_cls<P>(reinterpret_cast<const V *>(smem + in) + (ib[t] + pc), vr, vi);
+                const int op = S::pout(t), oq = S::qout(t);
+                const bool p_first = S::first_p(op) == t, q_first = S::first_q(oq) == t;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    // P side
+                    if (PIV == 0 && !SC) {
+                        if (p_first) { pr[c][op] = vr[c]; pi[c][op] = vi[c]; }
+                        else { pr[c][op] += vr[c]; pi[c][op] += vi[c]; }
+                    } else {
+                        const T k = (PIV == 1 && neg[c]) ? -pcf[t] : pcf[t];
+                        if (p_first) { pr[c][op] = k * vr[c]; pi[c][op] = k * vi[c]; }
+                        else { pr[c][op] = fmaT(k, vr[c], pr[c][op]); pi[c][op] = fmaT(k, vi[c], pi[c][op]); }
+                    }
+                    // Q side
+                    if (q_first) { qr[c][oq] = vr[c]; qi[c][oq] = vi[c]; }
+                    else if (PIV == 1) { qr[c][oq] += vr[c]; qi[c][oq] += vi[c]; }
+                    else { qr[c][oq] = fmaT(rel[t], vr[c], qr[c][oq]); qi[c][oq] = fmaT(rel[t], vi[c], qi[c][oq]); }
+                }
+            }
+#pragma unroll
+            for (int tau = 0; tau < 2; tau++) {
+                const bool hp = S::first_p(tau) >= 0, hq = S::first_q(tau) >= 0;
+                T orr[P], oii[P];
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    T bR = qbr[tau], bI = qbi[tau];
+                    if (PIV == 0 && neg[c]) { bR = -bR; bI = -bI; }
+                    T re, im;
+                    if (hp && hq) {
+                        re = fmaT(bR, qr[c][tau], fmaT(-bI, qi[c][tau], pr[c][tau]));
+                        im = fmaT(bR, qi[c][tau], fmaT(bI, qr[c][tau], pi[c][tau]));
+                    } else if (hp) {
+                        re = pr[c][tau];
+                        im = pi[c][tau];
+                    } else {
+                        re = fmaT(-bI, qi[c][tau], bR * qr[c][tau]);
+                        im = fmaT(bI, qr[c][tau], bR * qi[c][tau]);
+                    }
+                    orr[c] = re;
+                    oii[c] = im;
+                    nsum = fmaT(re, re, nsum);
+                    nsum = fmaT(im, im, nsum);
+                }
+                if (LAST) st_perm<P>(ob[tau], pc ^ ol[tau], orr, oii);
+                if (STS) sts_cls<P>(reinterpret_cast<V *>(smem + out) + (oidx[tau] + pc), orr, oii);
+            }
+        }
+    }
+}
+
+// The packed two-lane FP32 form of group_cosets_f (the thread's two adjacent classes in the lanes of f32x2
+// registers; stages between steps as (re0, re1, im0, im1)).
+template <int NTQ, int H, int PIV, bool SC, bool FIRST, bool LAST, bool STS>
+__device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const GroupStepArgs &gs, float2 *__restrict__ mem,
+                                                 const uint64_t TB, const int L, const uint32_t in, const uint32_t out,
+                                                 const float sc, const float br, const float bi, float &nsum) {
+    typedef FShape<NTQ, H, PIV> S;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - 1;
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    float sg[NTQ];
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) sg[t] = gs.par[t] ? -1.f : 1.f;
+    f32x2 QBR[2], QBI[2], QBN[2], REL[NTQ], PCF[NTQ];
+#pragma unroll
+    for (int tau = 0; tau < 2; tau++) {
+        const int f = S::first_q(tau);
+        const float s = (PIV == 0 && f >= 0) ? sg[f < 0 ? 0 : f] : 1.f;
+        QBR[tau] = f2_pack(br * s, br * s);
+        QBI[tau] = f2_pack(bi * s, bi * s);
+        QBN[tau] = f2_pack(-bi * s, -bi * s);
+    }
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) {
+        const int f = S::first_q(S::qout(t));
+        const float rl = PIV == 0 ? sg[t] * sg[f < 0 ? 0 : f] : 1.f;
+        const float pk = PIV == 0 ? sc : sc * sg[t];
+        REL[t] = f2_pack(rl, rl);
+        PCF[t] = f2_pack(pk, pk);
+    }
+    const float sig1 = (lam & 1u) ? -1.f : 1.f;
+    const f32x2 SGP = f2_pack(1.f, sig1), SGN = f2_pack(-1.f, -sig1);
+    f32x2 NS = 0ull;
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t zl[NTQ], ib[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            ib[t] = (uint32_t)gs.in_idx[j][t] * NC;
+            zl[t] = FIRST ? ga.z0lo[j][t] : 0u;
+        }
+        uint32_t ol[2] = {0, 0}, oidx[2] = {0, 0};
+        float2 *ob[2] = {mem, mem};
+#pragma unroll
+        for (int tau = 0; tau < 2; tau++) {
+            oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
+            ol[tau] = LAST ? ga.zdlo[j][tau] : 0u;
+            if (LAST) ob[tau] = mem + (TB ^ ga.blk_out[gs.out_idx[j][tau]]);
+        }
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = 2u * g;
+            const f32x2 SG = ((mp ^ __popc(pc & lam)) & 1) ? SGN : SGP;
+            f32x2 PR[2], PI[2], QR[2], QI[2];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                f32x2 VR, VI;
+                if (FIRST) {
+                    const float2 *src = reinterpret_cast<const float2 *>(smem + in) + ib[t];
+                    const uint32_t pos = pc ^ zl[t];
+                    const float2 a = src[pos], b = src[pos ^ 1u];
+                    VR = f2_pack(a.x, b.x);
+                    VI = f2_pack(a.y, b.y);
+                } else {
+                    const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib[t] + pc));
+                    VR = f2_pack(v.x, v.y);
+                    VI = f2_pack(v.z, v.w);
+                }
+                const int op = S::pout(t), oq = S::qout(t);
+                const bool p_first = S::first_p(op) == t, q_first = S::first_q(oq) == t;
+                if (PIV == 0 && !SC) {
+                    if (p_first) { PR[op] = VR; PI[op] = VI; }
+                    else { PR[op] = f2_add(PR[op], VR); PI[op] = f2_add(PI[op], VI); }
+                } else {
+                    const f32x2 K = PIV == 1 ? f2_mul(SG, PCF[t]) : PCF[t];
+                    if (p_first) { PR[op] = f2_mul(K, VR); PI[op] = f2_mul(K, VI); }
+                    else { PR[op] = f2_fma(K, VR, PR[op]); PI[op] = f2_fma(K, VI, PI[op]); }
+                }
+                if (q_first) { QR[oq] = VR; QI[oq] = VI; }
+                else if (PIV == 1) { QR[oq] = f2_add(QR[oq], VR); QI[oq] = f2_add(QI[oq], VI); }
+                else { QR[oq] = f2_fma(REL[t], VR, QR[oq]); QI[oq] = f2_fma(REL[t], VI, QI[oq]); }
+            }
+#pragma unroll
+            for (int tau = 0; tau < 2; tau++) {
+                const bool hp = S::first_p(tau) >= 0, hq = S::first_q(tau) >= 0;
+                f32x2 BR = QBR[tau], BI = QBI[tau], BN = QBN[tau];
+                if (PIV == 0) { BR = f2_mul(SG, BR); BI = f2_mul(SG, BI); BN = f2_mul(SG, BN); }
+                f32x2 RE, IM;
+                if (hp && hq) {
+                    RE = f2_fma(BR, QR[tau], f2_fma(BN, QI[tau], PR[tau]));
+                    IM = f2_fma(BR, QI[tau], f2_fma(BI, QR[tau], PI[tau]));
+                } else if (hp) {
+                    RE = PR[tau];
+                    IM = PI[tau];
+                } else {
+                    RE = f2_fma(BN, QI[tau], f2_mul(BR, QR[tau]));
+                    IM = f2_fma(BI, QR[tau], f2_mul(BR, QI[tau]));
+                }
+                NS = f2_fma(RE, RE, NS);
+                NS = f2_fma(IM, IM, NS);
+                if (LAST || STS) {
+                    float r0, r1, i0, i1;
+                    f2_unpack(RE, r0, r1);
+                    f2_unpack(IM, i0, i1);
+                    if (LAST) {
+                        const uint32_t pos = pc ^ ol[tau];
+                        ob[tau][pos] = make_float2(r0, i0);
+                        ob[tau][pos ^ 1u] = make_float2(r1, i1);
+                    }
+                    if (STS)
+                        *reinterpret_cast<float4 *>(reinterpret_cast<float2 *>(smem + out) + (oidx[tau] + pc)) =
+                            make_float4(r0, r1, i0, i1);
+                }
+            }
+        }
+    }
+    float a, b;
+    f2_unpack(NS, a, b);
+    nsum += a + b;
+}
+
 template <typename E, typename T, bool FIRST, bool LAST, bool STS, int NB, int NR, bool PK>
 __device__ __forceinline__ void group_cosets_any(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
                                                  const uint64_t TB, const int L, const uint32_t (&in)[NB],
@@ -581,6 +875,229 @@ __device__ __forceinline__ void group_cosets_any(const GroupArgs &ga, const Grou
     }
 }
 
+// ---------------------------------------------------------------------------------------------------------------
+// Trailing step of a complex64 sampling pass by shared sums.  Both branch norms of the next step,
+//   n(b) = sum |M[b][0] S0 + M[b][1] Z|^2 = |M[b][0]|^2 A + |M[b][1]|^2 B + 2 Re(M[b][0] conj(M[b][1]) C),
+// need only A = sum |S0|^2, B = sum |Z|^2 and C = sum S0 conj(Z) (Z = s_c S1, the signed x = 1 sum), about half the
+// arithmetic of rotating by both rows.  acc = (A, B, Re C, Im C).  n(b) then carries an absolute error of order
+// eps (A + B) instead of a relative one; n(0) + n(1) = A + B has none (M is unitary), so the bit decision is as
+// good, and the log2 Pr of the chosen branch is taken from the norm the next pass writes (group_decide / k_group).
+template <typename E, typename T, int P, int NTQ, int H>
+__device__ __forceinline__ void group_trail_abc(const GroupArgs &ga, const GroupStepArgs &gs, const uint64_t TB,
+                                                const int L, const uint32_t in, T (&acc)[4]) {
+    typedef typename CplxOf<T>::type V;
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - (P == 2 ? 1 : 0);
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    T sg[NTQ];
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) sg[t] = gs.par[t] ? (T)-1 : (T)1;
+    typedef FShape<NTQ, H, 0> S;   // pout = output of the x = 0 term, qout = output of the x = 1 term
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t ib[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) ib[t] = (uint32_t)gs.in_idx[j][t] * NC;
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = (uint32_t)P * g;
+            T xr[P][2], xi[P][2], zr[P][2], zi[P][2];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                T vr[P], vi[P];
+                lds_cls<P>(reinterpret_cast<const V *>(smem + in) + (ib[t] + pc), vr, vi);
+                const int o0 = S::pout(t), o1 = S::qout(t);
+                const bool f0 = S::first_p(o0) == t, f1 = S::first_q(o1) == t;
+#pragma unroll
+                for (int c = 0; c < P; c++) {
+                    if (f0) { xr[c][o0] = vr[c]; xi[c][o0] = vi[c]; }
+                    else { xr[c][o0] += vr[c]; xi[c][o0] += vi[c]; }
+                    if (f1) { zr[c][o1] = sg[t] * vr[c]; zi[c][o1] = sg[t] * vi[c]; }
+                    else { zr[c][o1] = fmaT(sg[t], vr[c], zr[c][o1]); zi[c][o1] = fmaT(sg[t], vi[c], zi[c][o1]); }
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < P; c++) {
+                const bool neg = ((mp ^ __popc(pc & lam) ^ __popc((uint32_t)c & lam)) & 1) != 0;
+                const T s = neg ? (T)-1 : (T)1;
+#pragma unroll
+                for (int tau = 0; tau < 2; tau++) {
+                    const bool h0 = S::first_p(tau) >= 0, h1 = S::first_q(tau) >= 0;
+                    if (h0) acc[0] = fmaT(xr[c][tau], xr[c][tau], fmaT(xi[c][tau], xi[c][tau], acc[0]));
+                    if (h1) acc[1] = fmaT(zr[c][tau], zr[c][tau], fmaT(zi[c][tau], zi[c][tau], acc[1]));
+                    if (h0 && h1) {
+                        // C += s_c (x0 conj(z1))
+                        const T cr = fmaT(xr[c][tau], zr[c][tau], xi[c][tau] * zi[c][tau]);
+                        const T ci = fmaT(xi[c][tau], zr[c][tau], -xr[c][tau] * zi[c][tau]);
+                        acc[2] = fmaT(s, cr, acc[2]);
+                        acc[3] = fmaT(s, ci, acc[3]);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// The packed two-lane FP32 form (stage layout (re0, re1, im0, im1)).
+template <int NTQ, int H>
+__device__ __forceinline__ void group_trail_abc_pk(const GroupArgs &ga, const GroupStepArgs &gs, const uint64_t TB,
+                                                   const int L, const uint32_t in, float (&acc)[4]) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - 1;
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    typedef FShape<NTQ, H, 0> S;
+    f32x2 SGT[NTQ];
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) {
+        const float v = gs.par[t] ? -1.f : 1.f;
+        SGT[t] = f2_pack(v, v);
+    }
+    const float sig1 = (lam & 1u) ? -1.f : 1.f;
+    const f32x2 SGP = f2_pack(1.f, sig1), SGN = f2_pack(-1.f, -sig1);
+    f32x2 AA = 0ull, BB = 0ull, CR = 0ull, CI = 0ull;
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t ib[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) ib[t] = (uint32_t)gs.in_idx[j][t] * NC;
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = 2u * g;
+            f32x2 XR[2], XI[2], ZR[2], ZI[2];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib[t] + pc));
+                const f32x2 VR = f2_pack(v.x, v.y), VI = f2_pack(v.z, v.w);
+                const int o0 = S::pout(t), o1 = S::qout(t);
+                const bool f0 = S::first_p(o0) == t, f1 = S::first_q(o1) == t;
+                if (f0) { XR[o0] = VR; XI[o0] = VI; }
+                else { XR[o0] = f2_add(XR[o0], VR); XI[o0] = f2_add(XI[o0], VI); }
+                if (f1) { ZR[o1] = f2_mul(SGT[t], VR); ZI[o1] = f2_mul(SGT[t], VI); }
+                else { ZR[o1] = f2_fma(SGT[t], VR, ZR[o1]); ZI[o1] = f2_fma(SGT[t], VI, ZI[o1]); }
+            }
+            const f32x2 SG = ((mp ^ __popc(pc & lam)) & 1) ? SGN : SGP;
+#pragma unroll
+            for (int tau = 0; tau < 2; tau++) {
+                const bool h0 = S::first_p(tau) >= 0, h1 = S::first_q(tau) >= 0;
+                if (h0) AA = f2_fma(XR[tau], XR[tau], f2_fma(XI[tau], XI[tau], AA));
+                if (h1) BB = f2_fma(ZR[tau], ZR[tau], f2_fma(ZI[tau], ZI[tau], BB));
+                if (h0 && h1) {
+                    const f32x2 SZR = f2_mul(SG, ZR[tau]), SZI = f2_mul(SG, ZI[tau]);
+                    CR = f2_fma(XR[tau], SZR, f2_fma(XI[tau], SZI, CR));
+                    CI = f2_fma(XI[tau], SZR, f2_fma(f2_mul(XR[tau], f2_pack(-1.f, -1.f)), SZI, CI));
+                }
+            }
+        }
+    }
+    float a, b;
+    f2_unpack(AA, a, b); acc[0] += a + b;
+    f2_unpack(BB, a, b); acc[1] += a + b;
+    f2_unpack(CR, a, b); acc[2] += a + b;
+    f2_unpack(CI, a, b); acc[3] += a + b;
+}
+
+template <typename E, typename T, bool PK>
+__device__ __forceinline__ void group_trail64(const GroupArgs &ga, const GroupStepArgs &gs, const uint64_t TB,
+                                              const int L, const uint32_t in, T (&acc)[4]) {
+    if constexpr (PK) {
+#define GSB_GT(NTQ_, H_) group_trail_abc_pk<NTQ_, H_>(ga, gs, TB, L, in, acc)
+        switch (gs.kind) {
+            case GK_1_0: GSB_GT(1, 0); break;
+            case GK_2_0: GSB_GT(2, 0); break;
+            case GK_2_1: GSB_GT(2, 1); break;
+            case GK_4_0: GSB_GT(4, 0); break;
+            case GK_4_1: GSB_GT(4, 1); break;
+            default: GSB_GT(4, 2); break;
+        }
+#undef GSB_GT
+    } else {
+#define GSB_GT(NTQ_, H_) group_trail_abc<E, T, 2, NTQ_, H_>(ga, gs, TB, L, in, acc)
+        switch (gs.kind) {
+            case GK_1_0: GSB_GT(1, 0); break;
+            case GK_2_0: GSB_GT(2, 0); break;
+            case GK_2_1: GSB_GT(2, 1); break;
+            case GK_4_0: GSB_GT(4, 0); break;
+            case GK_4_1: GSB_GT(4, 1); break;
+            default: GSB_GT(4, 2); break;
+        }
+#undef GSB_GT
+    }
+}
+
+// A written step of a complex64 pass: the factored form when the step has a compile-time shape and a pivot (piv >= 0,
+// GroupStepArgs::piv), else the general form with the scaled M row (w_r, w_i).
+template <typename T, bool SC, bool FIRST, bool LAST, bool STS, bool PK>
+__device__ __forceinline__ void group_written64(const GroupArgs &ga, const GroupStepArgs &gs, float2 *__restrict__ mem,
+                                                const uint64_t TB, const int L, const uint32_t in, const uint32_t out,
+                                                const int piv, const T sc, const T br, const T bi,
+                                                const T (&w_r)[1][2], const T (&w_i)[1][2], T &nsum) {
+    if (piv >= 0 && gs.kind != GK_ANY) {
+        if constexpr (PK) {
+            static_assert(std::is_same<T, float>::value, "packed form: FP32 arithmetic");
+#define GSB_GF(NTQ_, H_, P_) group_cosets_pkf<NTQ_, H_, P_, SC, FIRST, LAST, STS>(ga, gs, mem, TB, L, in, out, sc, br, bi, nsum)
+            switch (gs.kind * 2 + piv) {
+                case GK_1_0 * 2: GSB_GF(1, 0, 0); break;
+                case GK_1_0 * 2 + 1: GSB_GF(1, 0, 1); break;
+                case GK_2_0 * 2: GSB_GF(2, 0, 0); break;
+                case GK_2_0 * 2 + 1: GSB_GF(2, 0, 1); break;
+                case GK_2_1 * 2: GSB_GF(2, 1, 0); break;
+                case GK_2_1 * 2 + 1: GSB_GF(2, 1, 1); break;
+                case GK_4_0 * 2: GSB_GF(4, 0, 0); break;
+                case GK_4_0 * 2 + 1: GSB_GF(4, 0, 1); break;
+                case GK_4_1 * 2: GSB_GF(4, 1, 0); break;
+                case GK_4_1 * 2 + 1: GSB_GF(4, 1, 1); break;
+                case GK_4_2 * 2: GSB_GF(4, 2, 0); break;
+                default: GSB_GF(4, 2, 1); break;
+            }
+#undef GSB_GF
+        } else {
+#define GSB_GF(NTQ_, H_, P_) group_cosets_f<float2, T, 2, NTQ_, H_, P_, SC, FIRST, LAST, STS>(ga, gs, mem, TB, L, in, out, sc, br, bi, nsum)
+            switch (gs.kind * 2 + piv) {
+                case GK_1_0 * 2: GSB_GF(1, 0, 0); break;
+                case GK_1_0 * 2 + 1: GSB_GF(1, 0, 1); break;
+                case GK_2_0 * 2: GSB_GF(2, 0, 0); break;
+                case GK_2_0 * 2 + 1: GSB_GF(2, 0, 1); break;
+                case GK_2_1 * 2: GSB_GF(2, 1, 0); break;
+                case GK_2_1 * 2 + 1: GSB_GF(2, 1, 1); break;
+                case GK_4_0 * 2: GSB_GF(4, 0, 0); break;
+                case GK_4_0 * 2 + 1: GSB_GF(4, 0, 1); break;
+                case GK_4_1 * 2: GSB_GF(4, 1, 0); break;
+                case GK_4_1 * 2 + 1: GSB_GF(4, 1, 1); break;
+                case GK_4_2 * 2: GSB_GF(4, 2, 0); break;
+                default: GSB_GF(4, 2, 1); break;
+            }
+#undef GSB_GF
+        }
+        return;
+    }
+    const uint32_t i1[1] = {in}, o1[1][1] = {{out}};
+    T ns1[1][1] = {{0}};
+    group_cosets_any<float2, T, FIRST, LAST, STS, 1, 1, PK>(ga, gs, mem, TB, L, i1, o1, w_r, w_i, ns1);
+    nsum += ns1[0][0];
+}
+
 // Bits of a sampling pass ('sample' / 'prob': the normalised two-pass chain, gsamp2.cpp:39-55), decided at the start
 // of the pass.  Step k's branch norms n(b) = |L_k(b) T|^2 come from
 //   GSRC_TRAILING: the previous pass (it evaluated step k on the table it wrote: st->n0, st->n1);
@@ -609,9 +1126,15 @@ __device__ __forceinline__ bool group_decide(const GroupArgs &ga, const Ctx &cx,
         if (s == 0 && ga.src == GSRC_TRAILING) { n0 = st->n0; n1 = st->n1; }
         else if (s == 0) { n0 = ga.st[0].c[0] * st->prev; n1 = ga.st[0].c[1] * st->prev; }   // |T|^2 as stored
         else { n0 = ga.st[s].c[0]; n1 = ga.st[s].c[1]; }
-        const double p1 = n1 / (n0 + n1);
+        // shared-sum estimates (st->trx) are good to about TRX_FLOOR absolute in p1: a draw never takes a branch
+        // below that, and a forced branch is written with at least that estimate; the pass's written norm then
+        // gives the branch probability itself (k_group's epilogue)
+        const bool trx = s == 0 && ga.src == GSRC_TRAILING && st->trx;
+        double p1 = n1 / (n0 + n1);
+        if (trx && !cx.forced) p1 = p1 < TRX_FLOOR ? 0.0 : p1 > 1 - TRX_FLOOR ? 1.0 : p1;
         const int b = cx.forced ? cx.forced[row + k] : (cx.unif[row + k] < p1);
-        const double pb = b ? p1 : 1 - p1;
+        double pb = b ? p1 : 1 - p1;
+        if (trx && cx.forced && pb < TRX_FLOOR) pb = TRX_FLOOR;
         if (!(pb > 0)) {
             if (rec) {
                 st->dead = 1;
@@ -621,7 +1144,7 @@ __device__ __forceinline__ bool group_decide(const GroupArgs &ga, const Ctx &cx,
             return false;
         }
         lp += log2(pb);
-        scale /= sqrt(b ? n1 : n0);
+        scale /= sqrt(trx ? pb * (n0 + n1) : (b ? n1 : n0));
         bv[s] = b;
         if (rec) cx.bits_out[row + k] = (int8_t)b;
     }
@@ -747,6 +1270,21 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             wj[s][0][x] = (T)(f * ga.st[s].Mi[bv][x]);
         }
     }
+    // complex64 arena: the factored coefficients of each written step (pivot, beta with the pass's scale, cp)
+    constexpr bool FACT = sizeof(E) == 8;
+    int fpiv[D];
+    T fsc[D], fbr[D], fbi[D];
+    double fcp[D];
+#pragma unroll
+    for (int s = 0; s < D; s++) {
+        const int bv = s_bv[s];
+        const double f = s == 0 ? s_sc : 1.0;
+        fpiv[s] = FACT ? ga.st[s].piv[bv] : -1;
+        fsc[s] = (T)f;
+        fbr[s] = (T)(f * ga.st[s].br[bv]);
+        fbi[s] = (T)(f * ga.st[s].bi[bv]);
+        fcp[s] = FACT ? ga.st[s].cp[bv] : 1.0;
+    }
     T tr_r[2][2], tr_i[2][2];   // trailing step: both rows
 #pragma unroll
     for (int b = 0; b < 2; b++)
@@ -755,7 +1293,10 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             tr_r[b][x] = TR ? (T)ga.st[D].Mr[b][x] : (T)0;
             tr_i[b][x] = TR ? (T)ga.st[D].Mi[b][x] : (T)0;
         }
-    constexpr int ND = D + 2 * TR;
+    // reduced sums: the written steps' norms, then (TR) the trailing step's (n0, n1, 0, 0), or its shared sums
+    // (A, B, Re C, Im C) when it takes the complex64 shared-sum form
+    constexpr int ND = D + 4 * TR;
+    const bool trail_abc = FACT && TR == 1 && ga.st[D].kind != GK_ANY;
     double acc[ND];
 #pragma unroll
     for (int s = 0; s < ND; s++) acc[s] = 0;
@@ -788,7 +1329,9 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
         for (int i = 0; i < ga.ssz[0]; i++) bulk_load(dst + (uint32_t)i * blk_bytes, mem + (TBn ^ ga.blk_in[i]), blk_bytes, bar);
     };
     int issued = 0;   // tiles whose loads thread 0 issued
-    if (threadIdx.x == 0 && !ga.withhold_loads)
+    // test hook: 1 withholds every CTA's tile loads, 2 only those of the odd CTAs (a partial failure)
+    const bool withhold = ga.withhold_loads == 1 || (ga.withhold_loads == 2 && (blockIdx.x & 1u));
+    if (threadIdx.x == 0 && !withhold)
         for (unsigned int n = i0; n < i1 && n < i0 + 2; n++) {
             issue_loads(n, tile_tb(n));
             issued++;
@@ -813,38 +1356,74 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
         const uint32_t tin[1] = {sm.in0 + (uint32_t)buf * sm.in_bytes};
         // written steps: the first reads the input tile, the last writes the arena (and keeps its stage for the
         // trailing step); the input buffer is free once the first step is done: tile it + 2 goes there
-        if (D == 1) {
+        if constexpr (FACT) {
+            float2 *m64 = reinterpret_cast<float2 *>(mem);
+            if (D == 1)
+                group_written64<T, true, true, true, TR == 1, PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
+                                                                 fsc[0], fbr[0], fbi[0], w[0], wj[0], ns[0][0][0]);
+            else
+                group_written64<T, true, true, false, true, PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
+                                                               fsc[0], fbr[0], fbi[0], w[0], wj[0], ns[0][0][0]);
+            __syncthreads();
+        } else if (D == 1) {
             group_cosets_any<E, T, true, true, TR == 1, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         } else {
             group_cosets_any<E, T, true, false, true, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
             __syncthreads();
         }
-        if (threadIdx.x == 0 && it + 2 < i1 && !ga.withhold_loads) {
+        if (threadIdx.x == 0 && it + 2 < i1 && !withhold) {
             // tile it + 2 is two Gray-code steps from this tile (gray(n + 1) = gray(n) ^ 2^ctz(n + 1)); rebuilding its
             // base from the index, a loop over the class-base vectors, held up warp 0 and so every warp at the next
             // barrier (4-7 % of the pass)
             issue_loads(it + 2, TB ^ ((ga.bhi[__ffs((int)(it + 1)) - 1] ^ ga.bhi[__ffs((int)(it + 2)) - 1]) & ~mask));
             issued++;
         }
-        if (D == 2) {
+        if constexpr (FACT) {
+            float2 *m64 = reinterpret_cast<float2 *>(mem);
+            if (D == 2) {
+                group_written64<T, false, false, true, TR == 1, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
+                                                                   fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
+                                                                   fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
+                                                                   w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
+            } else if (D == 3) {
+                group_written64<T, false, false, false, true, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
+                                                                 fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
+                                                                 fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
+                                                                 w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
+                __syncthreads();
+                group_written64<T, false, false, true, false, PK>(ga, ga.st[2], m64, TB, L, sm.mid[2], 0u,
+                                                                 fpiv[D > 2 ? 2 : 0], fsc[D > 2 ? 2 : 0],
+                                                                 fbr[D > 2 ? 2 : 0], fbi[D > 2 ? 2 : 0],
+                                                                 w[D > 2 ? 2 : 0], wj[D > 2 ? 2 : 0], ns[D > 2 ? 2 : 0][0][0]);
+            }
+        } else if (D == 2) {
             group_cosets_any<E, T, false, true, TR == 1, 1, 1, PK>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
         } else if (D == 3) {
             group_cosets_any<E, T, false, false, true, 1, 1, PK>(ga, ga.st[1], mem, TB, L, m1, m2o, w[1], wj[1], ns[1]);
             __syncthreads();
             group_cosets_any<E, T, false, true, false, 1, 1, PK>(ga, ga.st[2], mem, TB, L, m2, none1, w[2], wj[2], ns[2]);
         }
+        T tabc[4] = {0, 0, 0, 0};
         if (TR) {
             if (D > 1) __syncthreads();
             const uint32_t(&tmid)[1] = D == 1 ? m1 : m2;
-            group_cosets_any<E, T, false, false, false, 1, 2, PK>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
+            if (FACT && trail_abc)
+                group_trail64<E, T, PK>(ga, ga.st[D], TB, L, tmid[0], tabc);
+            else
+                group_cosets_any<E, T, false, false, false, 1, 2, PK>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
         }
         __syncthreads();
 #pragma unroll
         for (int s = 0; s < D; s++) acc[s] += (double)ns[s][0][0];
         if (TR) {
-            acc[D] += (double)nt[0][0];
-            acc[ND - 1] += (double)nt[0][1];
+            if (trail_abc) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) acc[TR ? D + i : 0] += (double)tabc[i];
+            } else {
+                acc[TR ? D : 0] += (double)nt[0][0];
+                acc[TR ? D + 1 : 0] += (double)nt[0][1];
+            }
         }
         if (it + 1 < i1) tb ^= ga.bhi[__ffs((int)(it + 1)) - 1] & ~mask;
     }
@@ -855,6 +1434,10 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             st->dead = 1;
             volatile int never = 0;
             for (int n = waited; n < issued; n++) mbar_wait_bounded(bar0 + 8 * (uint32_t)(n & 1), (uint32_t)(n >> 1) & 1, &never);
+            // count this block as finished, so the block that finishes last (a failed one or one in grid_reduceN)
+            // sees every block and returns the counter to zero
+            __threadfence();
+            if (atomicAdd(&st->counter, 1u) == gridDim.x - 1) st->counter = 0;
         }
         __syncthreads();
         return;
@@ -862,12 +1445,44 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
     double tot[ND];
     if (!grid_reduceN<ND>(acc, cx, tot)) return;
     if (cx.driver == DRV_CHAIN1) {
-        group_chain1_epilogue<D>(cx, ga.st[0].k, *reinterpret_cast<const double(*)[D]>(tot));
+        group_chain1_epilogue<D>(cx, ga.st[0].k, *reinterpret_cast<const double(*)[D]>(tot), fcp);
     } else {
+        if (ga.src == GSRC_TRAILING && st->trx) {
+            // the first bit came from shared-sum estimates: its branch probability is the estimate used times the
+            // ratio of the written norm to the one the pass's scale aimed at (1 / prod cp)
+            double cpp = 1;
+#pragma unroll
+            for (int s = 0; s < D; s++) cpp *= fcp[s];
+            const double ratio = tot[D - 1] * cpp;
+            if (!(ratio > 0)) {
+                const size_t row = (size_t)st->item * (size_t)cx.ns;
+                st->dead = 1;
+                st->logp = -INFINITY;
+                for (int j = ga.st[0].k; j < cx.ns; j++) cx.bits_out[row + j] = cx.forced ? cx.forced[row + j] : 0;
+                return;
+            }
+            st->logp += log2(ratio);
+        }
         st->prev = tot[D - 1];
+        st->trx = 0;
         if (TR) {
-            st->n0 = tot[D];
-            st->n1 = tot[ND - 1];
+            if (trail_abc) {
+                const GroupStepArgs &g = ga.st[D < 3 ? D : 0];
+                const double A = tot[TR ? D : 0], B = tot[TR ? D + 1 : 0], Cr = tot[TR ? D + 2 : 0], Ci = tot[TR ? D + 3 : 0];
+                double nb[2];
+                for (int b = 0; b < 2; b++) {
+                    const double a0 = g.Mr[b][0], b0 = g.Mi[b][0], a1 = g.Mr[b][1], b1 = g.Mi[b][1];
+                    const double v = (a0 * a0 + b0 * b0) * A + (a1 * a1 + b1 * b1) * B +
+                                     2 * ((a0 * a1 + b0 * b1) * Cr - (b0 * a1 - a0 * b1) * Ci);
+                    nb[b] = v > 0 ? v : 0;
+                }
+                st->n0 = nb[0];
+                st->n1 = nb[1];
+                st->trx = 1;
+            } else {
+                st->n0 = tot[TR ? D : 0];
+                st->n1 = tot[TR ? D + 1 : 0];
+            }
         }
     }
 }

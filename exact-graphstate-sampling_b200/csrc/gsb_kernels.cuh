@@ -48,6 +48,7 @@ struct DevState {
     int item;         // index of the string / sample being evaluated
     unsigned int counter;   // blocks finished in the current launch
     int err;                // a bounded pipeline wait gave up (reported to the host, cleared when read)
+    int trx;                // n0, n1 were expanded from a trailing step's shared sums (fused sampling passes)
 };
 
 struct Ctx {
@@ -601,6 +602,7 @@ __global__ void k_begin(E *mem, DevState *st) {
     st->dead = 0;
     st->counter = 0;
     st->aux = 0;
+    st->trx = 0;
 }
 
 // End of a string / sample: final log2 Pr, next item.

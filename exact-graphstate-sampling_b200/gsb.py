@@ -8,6 +8,7 @@ The library must be built (``python build.py``); there is no fallback: importing
 libgsb.so, or opening an engine without a CUDA device, raises.
 """
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -79,6 +80,8 @@ def _load():
         "gsb_pass_list": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_int), c.POINTER(c.c_int), c.POINTER(c.c_int),
                                     c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_test_withhold_tile_loads": (c.c_int, [P, c.c_int]),
+        "gsb_set_guard": (c.c_int, [P, P, c.c_double]),
+        "gsb_guard_evaluations": (c.c_int, [P, c.POINTER(c.c_int64)]),
         "gsb_autotune": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_batch_open": (c.c_int, [c.POINTER(c.c_char_p), c.POINTER(c.c_size_t), c.c_int, c.c_int, c.c_int,
                                      c.POINTER(P)]),
@@ -106,7 +109,7 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_probe_l2_copy", "gsb_test_withhold_tile_loads", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_probe_l2_copy", "gsb_test_withhold_tile_loads", "gsb_set_guard", "gsb_guard_evaluations", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
            "gsb_grad_run", "gsb_autotune", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
@@ -146,6 +149,27 @@ def as_bits(strings, ns, allow_free=False):
     if not allow_free and (a < 0).any():
         raise ValueError("'?' is only allowed in hybrid / resume strings")
     return a
+
+
+# Error model of the complex64 form (complex64 arena, FP32 arithmetic), measured against complex128 on the n = 70,
+# width-30 workload: the log2 Pr error of a string is close to normal with standard deviation
+#     sigma(x) = C64_SIGMA_STEP * sqrt(nsteps) / sqrt(x),   x = Pr * 2^nsteps,
+# since the rounding of the stored table is absolute in units of its norm and each step adds its own.
+C64_SIGMA_STEP = 8.1e-8
+C64_GUARD_Z = 5.5
+
+
+def c64_sigma(log2p, nsteps):
+    """Estimated standard deviation of a complex64 log2 Pr (the stated error of each result)."""
+    x = np.exp2(np.asarray(log2p, np.float64) + nsteps)
+    with np.errstate(divide="ignore"):
+        return C64_SIGMA_STEP * math.sqrt(nsteps) / np.sqrt(x)
+
+
+def c64_guard_log2_xmin(nsteps, tol=1e-5, z=C64_GUARD_Z):
+    """log2 of the probability ratio x = Pr 2^nsteps below which z standard deviations of the complex64 error
+    exceed tol: the threshold of Engine.set_guard for |d log2 Pr| <= tol."""
+    return 2.0 * math.log2(z * C64_SIGMA_STEP * math.sqrt(nsteps) / tol)
 
 
 class Engine:
@@ -328,10 +352,10 @@ class Engine:
         _check(_lib.gsb_fusion_groups(self.handle, _ptr(g, ctypes.c_int), _ptr(e, ctypes.c_double)))
         return [int(x) for x in g[:self.ns]], e[:self.ns]
 
-    def test_withhold_tile_loads(self, on):
-        """Test hook: the fused passes issue no tile loads, so their bounded waits run out and calls raise
-        GsbError (GSB_E_CUDA); off again, the engine runs normally."""
-        _check(_lib.gsb_test_withhold_tile_loads(self.handle, 1 if on else 0))
+    def test_withhold_tile_loads(self, on, partial=False):
+        """Test hook: the fused passes issue no tile loads (partial=True: only in their odd CTAs), so those CTAs'
+        bounded waits run out and calls raise GsbError (GSB_E_CUDA); off again, the engine runs normally."""
+        _check(_lib.gsb_test_withhold_tile_loads(self.handle, (2 if partial else 1) if on else 0))
 
     def sample_groups(self):
         """The sampling passes: (steps written per pass at its first step, 0 inside a pass; table entries read +
@@ -350,6 +374,17 @@ class Engine:
         _check(_lib.gsb_pass_list(self.handle, int(mode), n.value, *[_ptr(a, ctypes.c_int) for a in cols],
                                   ctypes.byref(n)))
         return [tuple(int(a[i]) for a in cols) for i in range(n.value)]
+
+    def set_guard(self, guard, log2_xmin):
+        """Re-evaluate this complex64 engine's unlikely strings (log2 Pr + nsteps < log2_xmin) on `guard`, a
+        complex128 Engine of the same plan (None detaches).  The guard must stay open while attached."""
+        _check(_lib.gsb_set_guard(self.handle, None if guard is None else guard.handle, float(log2_xmin)))
+        self._guard = guard          # keeps the guard alive as long as it is attached
+
+    def guard_evaluations(self):
+        n = ctypes.c_int64()
+        _check(_lib.gsb_guard_evaluations(self.handle, ctypes.byref(n)))
+        return n.value
 
     def set_arith(self, bits):
         """complex64 wide-step arithmetic: 32 (FP32 sums and rotation, default) or 64 (exact sums + FP64 rotation,

@@ -2,8 +2,9 @@
 
 Drop-in for the reference's ``doped_sampler.py`` (doped_sampler.py:1-77): same argv, same output lines, same
 random streams.  The reference runs its executor as a subprocess per string or proposal (:25-26, 46-47, 56, 69),
-each one re-parsing the plan and allocating the arena.  Here one ``gsb.Engine`` stays loaded, and slice plans reuse
-its arena by swapping their M matrices.
+each one re-parsing the plan and allocating the arena.  Here one ``gsb.Engine`` stays loaded, unsliced proposals
+go to it in batches (one C-ABI call per batch of proposals), and slice plans reuse its arena by swapping their M
+matrices.
 
   python hybrid_sampler.py sample <plan> <step_vertices.json> <nprop> <seed> <cap> <out.txt> [--m M]
   python hybrid_sampler.py score  <plan> <step_vertices.json> <strings.txt> <out.txt> [--qiskit]
@@ -85,32 +86,48 @@ class HybridSampler:
                 f.write(f"{s} {lp:.9f} {time.time() - t0:.1f}\n")
                 f.flush()
 
+    def _hybrid_batches(self, props, seed):
+        """Unsliced proposals evaluated BATCH at a time: one gsb_hybrid call per batch replays the hybrid graph for
+        every line back to back (no host round trip between proposals).  Line i of the call draws its '?' bits from
+        mt19937_64(seed * 1000003 + i), the stream the reference gives proposal i (doped_sampler.py:69).
+        Yields (bits, log2 Pr, conditionals, seconds per proposal of its batch) per proposal."""
+        for i0 in range(0, len(props), self.BATCH):
+            lines = [self.to_step_string(p, True) for p in props[i0:i0 + self.BATCH]]
+            t0 = time.time()
+            bits, lpv, cond = self.eng.hybrid(lines, seed * 1000003, first_line=i0)
+            dt = (time.time() - t0) / len(lines)
+            for j in range(len(lines)):
+                yield bits[j], float(lpv[j]), cond[j], dt
+
+    BATCH = 64
+
     def sample(self, nprop, seed, cap, out_path):
         rng = random.Random(seed)
         props = [[rng.randrange(2) for _ in range(self.ND)] for _ in range(nprop)]
         u = [rng.random() for _ in range(nprop)]
         K = self.ns - self.m_suffix
         zmax, acc = 0.0, 0
+        batched = None if self.slices else self._hybrid_batches(props, seed)
         with open(out_path, "a") as f:
             f.write(f"# seed {seed} cap {cap} m_suffix {self.m_suffix} K {K} nprop {nprop}\n")
             for i in range(nprop):
                 t0 = time.time()
-                line = self.to_step_string(props[i], True)
-                lseed = seed * 1000003 + i
                 if self.slices:
-                    bits, lp_full, lp_prefix, _ = self.sliced_eval(line, lseed)
+                    line = self.to_step_string(props[i], True)
+                    bits, lp_full, lp_prefix, _ = self.sliced_eval(line, seed * 1000003 + i)
                     lp_full += self.NA
                     lp_prefix += self.NA
+                    dt = time.time() - t0
                 else:
-                    bits, lpv, cond = self.eng.hybrid([line], lseed)
-                    bits, lp_full, cond = bits[0], float(lpv[0]) + self.NA, cond[0]
+                    bits, lp_full, cond, dt = next(batched)
+                    lp_full += self.NA
                     lp_prefix = (sum(math.log2(c) for c in cond[:K]) + self.NA) if all(c > 0 for c in cond[:K]) else -math.inf
                 bits_step = "".join(str(int(x)) for x in bits)
                 z = 2.0 ** (lp_prefix + (self.ND - self.m_suffix))
                 zmax = max(zmax, z)
                 ok = u[i] < z / cap
                 b = "".join(bits_step[self.pos[q]] for q in range(self.ND))
-                f.write(f"{'ACC' if ok else 'rej'} {b} {lp_full:.9f} z={z:.6f} {time.time() - t0:.1f}s"
+                f.write(f"{'ACC' if ok else 'rej'} {b} {lp_full:.9f} z={z:.6f} {dt:.1f}s"
                         f"{' Z_ABOVE_CAP' if z > cap else ''}\n")
                 f.flush()
                 acc += ok

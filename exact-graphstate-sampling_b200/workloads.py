@@ -48,15 +48,29 @@ def rotation_instance(n, depth=None, seed=0, order_seed=12, iters=60000):
                 theta0=theta0, step_vertices=[int(x["v"]) for x in st])
 
 
-def batch_workload(count=512, seed=0, nmin=16, nmax=40, npre=16, nsuf=4, iters=5000):
+def qubit_order_instance(n, depth, seed):
+    """The matching construction with the qubits eliminated in index order (no order search): widths near n / 2."""
+    n, body, tail = circuits.matching_circuit(n, depth, seed=seed)
+    order = list(range(n))
+    text, st, R = build(n, body, tail, order)
+    return dict(name=f"matching_n{n}_d{depth}_s{seed}_qubit_order", n=n, body=body, tail=tail, order=order, width=R,
+                plan=text, steps=st)
+
+
+def batch_workload(count=512, seed=0, nmin=16, nmax=40, npre=16, nsuf=4, iters=5000, order="qubit"):
     """The batched workload: `count` matching instances with n uniform in [nmin, nmax] (instance i: circuit seed
-    seed * 100003 + i, order seed 12), and per instance npre random prefixes over its first floor(ns/2) steps, each
-    with nsuf random suffixes.  Returns dict(instances, K, prefixes, suffixes)."""
+    seed * 100003 + i), and per instance npre random prefixes over its first floor(ns/2) steps, each with nsuf random
+    suffixes.  order "qubit" eliminates the qubits in index order (widths 7-20 for n in [16, 40], the widths the
+    batched configuration states); "search" uses the native order search (seed 12, `iters` moves: widths 4-17).
+    Returns dict(instances, K, prefixes, suffixes)."""
     rng = np.random.default_rng(seed)
     ns_list = rng.integers(nmin, nmax + 1, size=count)
     inst, K, pre, suf = [], [], [], []
     for i, n in enumerate(ns_list):
-        w = matching_instance(int(n), int(n), seed * 100003 + i, 12, iters)
+        if order == "qubit":
+            w = qubit_order_instance(int(n), int(n), seed * 100003 + i)
+        else:
+            w = matching_instance(int(n), int(n), seed * 100003 + i, 12, iters)
         ns = len(w["steps"])
         k = ns // 2
         inst.append(w)
@@ -77,11 +91,16 @@ def wide34_instance():
     return dict(name="matching_n80_d80_s6_w34", n=n, body=body, tail=tail, order=order, width=R, plan=text, steps=st)
 
 
-def wide34_slices(w, S=(0, 3, 2), order_seed=5, iters=60000):
+WIDE34_SLICES = (4, 59, 18, 60, 67, 39, 41, 10, 2, 26)
+
+
+def wide34_slices(w, S=WIDE34_SLICES, order_seed=5, iters=60000):
     """The width-34 instance's complex128 cross-check: a second order for the graph with the slice vertices S cut out
-    (native search, seed 5: width 33 for S = (0, 3, 2), so a 2^33-entry complex128 arena, 137 GB, fits), and the
-    reference-format slice plans of make_sliced_plans on it, one per assignment of S.  Every slice vertex and all of
-    their neighbours are eliminated by the last step, so the slices' final tables add up with no twist."""
+    (native search, seed 5), and the reference-format slice plans of make_sliced_plans on it, one per assignment of
+    S.  The default S, ten vertices picked greedily (each the vertex whose removal lowers the widest cuts of the
+    current order most), gives width 30: 1,024 slices, each a 2^30-entry complex128 arena (17.2 GB).  Every slice
+    vertex and all of their neighbours are eliminated by the last step, so the slices' final tables add up with no
+    twist."""
     import os
     import tempfile
     from graphform import graph_form

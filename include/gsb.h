@@ -150,6 +150,19 @@ int gsb_set_matrices(gsb_engine *e, const double *M);
  * Either way the stored table is complex64.  No effect on a complex128 engine. */
 int gsb_set_arith(gsb_engine *e, int bits);
 
+/* Complex128 re-evaluation of unlikely strings (no counterpart in the reference).  A complex64 log2 Pr carries a
+ * rounding error that grows like 1 / sqrt(x), x = Pr * 2^nsteps: the stored table's rounding is absolute in units
+ * of its norm, and an unlikely string's amplitude is a small remainder of it.  With a complex128 engine `g` of the
+ * same plan (same steps and matrices) attached to the complex64 engine `e`, every string of gsb_chain, gsb_prob,
+ * gsb_chain_device, gsb_sample, gsb_sample_uniform and gsb_sample_device whose complex64 result has
+ * log2 Pr + nsteps < log2_xmin (or is -inf) is evaluated again on `g`, and that result replaces it (a sample keeps
+ * its bits; its log2 Pr is re-evaluated).  Both engines must stay open while attached (closing either detaches);
+ * g = NULL detaches.  Errors: GSB_E_USAGE when e is not complex64, g not complex128, on another device, already
+ * guarding another engine, or of another plan. */
+int gsb_set_guard(gsb_engine *e, gsb_engine *g, double log2_xmin);
+/* Strings the guard of e re-evaluated since it was set. */
+int gsb_guard_evaluations(const gsb_engine *e, int64_t *count);
+
 /* Per-step kernel timing for one forced string: ms_write[k] and ms_norm[k] (0 when a pass does not run) from CUDA
  * events on the engine's stream, mode 0 = 'chain' (one pass per step), 1 = 'prob' (norm + write per step). */
 int gsb_profile_steps(gsb_engine *e, const int8_t *bits, int mode, float *ms_write, float *ms_norm);
@@ -216,10 +229,11 @@ int gsb_batch_get_shape(const gsb_batch *b, int *block, int *small_R, int *per_s
  * keeps the fastest; returns it and its mean time. */
 int gsb_batch_tune(gsb_batch *b, int reps, size_t max_bytes, int *block, int *small_R, int *per_sm, float *best_ms);
 
-/* Test hook for the fused passes' failure path (no counterpart in the reference): with on != 0 the passes issue no
- * tile loads, so every CTA's bounded wait runs out (about one second); the kernel records the failure, marks the
- * item dead and returns, and the call reports GSB_E_CUDA.  Nothing faults or hangs and the engine stays usable; with
- * on = 0 the passes run normally again. */
+/* Test hook for the fused passes' failure path (no counterpart in the reference): with on = 1 the passes issue no
+ * tile loads, so every CTA's bounded wait runs out (about one second); with on = 2 only the odd CTAs are starved
+ * (a partial failure: the other CTAs finish their tiles).  A starved CTA records the failure, marks the item dead,
+ * counts itself as finished and returns, and the call reports GSB_E_CUDA.  Nothing faults or hangs and the engine
+ * stays usable; with on = 0 the passes run normally again.  Other values: GSB_E_USAGE. */
 int gsb_test_withhold_tile_loads(gsb_engine *e, int on);
 
 /* ---- host-side helpers (no GPU needed) ---- */

@@ -10,10 +10,11 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def small_batch():
+@pytest.fixture(scope="module", params=["search", "qubit"])
+def small_batch(request):
     import workloads
-    return workloads.batch_workload(count=14, seed=3, nmin=16, nmax=30, npre=3, nsuf=2, iters=2000)
+    return workloads.batch_workload(count=14, seed=3, nmin=16, nmax=30, npre=3, nsuf=2, iters=2000,
+                                    order=request.param)
 
 
 def _strings(bw, i):
@@ -104,3 +105,36 @@ def test_l2_probe_measures_a_copy_bandwidth():
     import gsb
     gbs = gsb.probe_l2_copy(mib=24, reps=100)
     assert 2000.0 < gbs < 1e6, gbs
+
+
+def test_batch_vs_oracle(small_batch, tmp_path):
+    """Both precisions of the batched launch against the oracle's chain (the reference executor's restatement) on
+    every string of every instance: complex128 <= 1e-9; complex64 within 6 standard deviations of the complex64
+    error model (gsb.c64_sigma) and <= 1e-5 where that model allows it."""
+    import gsb
+    from oracle import Oracle
+    bw = small_batch
+    plans = [w["plan"] for w in bw["instances"]]
+    out = {}
+    for prec in (gsb.GSB_C128, gsb.GSB_C64):
+        b = gsb.Batch(plans, precision=prec)
+        b.set_strings(bw["K"], bw["prefixes"], bw["suffixes"])
+        out[prec] = b.run()[0]
+        b.close()
+    for i, w in enumerate(bw["instances"]):
+        path = tmp_path / f"p{i}.txt"
+        path.write_text(w["plan"])
+        o = Oracle(str(path), 128)
+        want = np.array([o.chain1(s)[0] for s in _strings(bw, i)])
+        o.close()
+        ns = len(w["steps"])
+        fin = np.isfinite(want)
+        got128 = out[gsb.GSB_C128][i].reshape(-1)
+        got64 = out[gsb.GSB_C64][i].reshape(-1)
+        assert (np.isfinite(got128) == fin).all()
+        assert np.max(np.abs(got128[fin] - want[fin]), initial=0.0) <= 1e-9
+        sig = gsb.c64_sigma(want[fin], ns)
+        d64 = np.abs(got64[fin] - want[fin])
+        assert (d64 <= 6 * sig).all(), (i, float(d64.max()))
+        ok = 6 * sig <= 1e-5
+        assert np.max(d64[ok], initial=0.0) <= 1e-5

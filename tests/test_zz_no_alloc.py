@@ -32,6 +32,24 @@ def test_extend_static_equals_extend_on_two_calls():
 
 
 @pytest.mark.gpu
+def test_extend_static_allocates_no_device_memory():
+    """After the first call on the device (which looks up the scratch's address), further calls leave the device's
+    free memory exactly as it was: they allocate nothing."""
+    import torch
+    import gsb
+    rng = np.random.default_rng(11)
+    old, piv, ker, rho, wv = _case(rng, 14, 14, 1)
+    gsb.dp_extend_static(old, 14, 14, rho, piv, ker, wv)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(3):
+        gsb.dp_extend_static(old, 14, 14, rho, piv, ker, wv)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, (free0, free1)
+
+
+@pytest.mark.gpu
 def test_extend_static_rejects_tables_beyond_its_scratch():
     import gsb
     rng = np.random.default_rng(5)
