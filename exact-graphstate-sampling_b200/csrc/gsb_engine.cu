@@ -153,6 +153,8 @@ struct Engine {
     int arith = 32;                      // arithmetic of the complex64 wide-step kernels: 32 (FP32) or 64 (FP64)
     int fuse_depth = 2;                  // chain mode: largest number of DP steps fused into one pass (1 = none)
     std::vector<Op> chain_ops;           // 'chain' passes
+    int hyb_K = 0;                       // gsb_set_hybrid_prefix: hybrid strings force their first hyb_K steps
+    std::vector<Op> hyb_ops;             // fused 'chain' passes over those steps
     std::vector<Op> sample_ops;          // 'prob' / 'sample' passes (build_sample_ops)
     int withhold_loads = 0;              // test hook: fused passes issue no tile loads (their bounded waits run out)
     std::vector<OpShape> chain_shapes;   // pass lists chosen by gsb_autotune (empty: the byte-model defaults)
@@ -177,6 +179,14 @@ struct Engine {
     Engine *guard = nullptr, *guarded = nullptr;
     double guard_lx = 0;
     int64_t guard_evals = 0;
+    // FP32 coefficients of a complex64 engine with FP32 arithmetic (apply_coeffs): per step, the M entries and the
+    // factored steps' pivot and ratio, rounded to float values
+    struct Coef32 {
+        double Mr[2][2], Mi[2][2];
+        int piv[2];
+        double br[2], bi[2], cp[2];
+    };
+    std::vector<Coef32> c32;
 
     ~Engine() {
         if (guard) guard->guarded = nullptr;
@@ -312,7 +322,18 @@ struct Engine {
             k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
             return cudaGetLastError();
         }
-        for (int k = 0; k < plan.ns; k++) {
+        int k0 = 0;
+        if (driver == DRV_HYBRID && hyb_K > 0) {
+            // forced prefix: 'chain' passes (fused where possible), then the run_steps state for the sampled steps
+            for (const Op &op : hyb_ops) {
+                e = launch_op(op, DRV_CHAIN1);
+                if (e != cudaSuccess) return e;
+            }
+            k_hybrid_switch<<<1, 1, 0, stream>>>(st, d_forced, d_bits, plan.ns, hyb_K);
+            if ((e = cudaGetLastError()) != cudaSuccess) return e;
+            k0 = hyb_K;
+        }
+        for (int k = k0; k < plan.ns; k++) {
             if (driver != DRV_CHAIN1) {
                 e = launch_step(k, false, driver, plan.ns, use_forced, use_unif);
                 if (e != cudaSuccess) return e;
@@ -356,6 +377,78 @@ struct Engine {
     }
 };
 
+// Float rounding of the FP32 kernels' coefficients by error diffusion.  A rounded coefficient c' = c (1 + d)
+// scales every amplitude path through it; the real part of d biases log2 Pr, the same way for every string, and
+// with round-to-nearest a plan whose steps repeat one matrix (a circuit with one rotation on every qubit) adds
+// those biases up step after step.  Each value is therefore rounded up or down (either is within one ulp) so that
+// the running sum of Re d over the steps, per coefficient role, stays within about one ulp of zero.
+static std::complex<double> round_diffused(std::complex<double> v, double &cum) {
+    if (v == 0.0) return v;
+    auto pair = [](double x, float &lo, float &hi) {
+        const float f = (float)x;
+        if ((double)f == x) { lo = hi = f; return; }
+        if ((double)f > x) { hi = f; lo = std::nextafter(f, -INFINITY); }
+        else { lo = f; hi = std::nextafter(f, INFINITY); }
+    };
+    float rl, rh, il, ih;
+    pair(v.real(), rl, rh);
+    pair(v.imag(), il, ih);
+    std::complex<double> best = v;
+    double bd = 0, bs = INFINITY;
+    for (int a = 0; a < 2; a++)
+        for (int b = 0; b < 2; b++) {
+            const std::complex<double> c((double)(a ? rh : rl), (double)(b ? ih : il));
+            const double d = ((c - v) / v).real();
+            const double sc = std::fabs(cum + d) + 1e-3 * std::abs((c - v) / v);   // ties: the nearer value
+            if (sc < bs) { bs = sc; best = c; bd = d; }
+        }
+    cum += bd;
+    return best;
+}
+
+// The coefficients a complex64 engine with FP32 arithmetic uses: M entries (single-step kernels, the fused passes'
+// general shape) and, per bit, the factored step's pivot (the larger of the row's two entries), its ratio
+// beta = M[b][1-piv] / M[b][piv] and cp = |M[b][piv]|^2 (exact), all rounded by round_diffused in step order.
+// Other engines use the plan's M as it is (FP64 arithmetic, or complex128).
+static void apply_coeffs(Engine &E) {
+    const HPlan &p = E.plan;
+    const bool f32 = E.prec == 64 && E.arith == 32;
+    E.c32.assign((size_t)p.ns, Engine::Coef32());
+    double cum_m[2][2] = {{0, 0}, {0, 0}}, cum_b[2] = {0, 0};
+    for (int k = 0; k < p.ns; k++) {
+        const HStep &hs = p.st[(size_t)k];
+        Engine::Coef32 &c = E.c32[(size_t)k];
+        for (int b = 0; b < 2; b++) {
+            for (int x = 0; x < 2; x++) {
+                std::complex<double> m(hs.Mr[b][x], hs.Mi[b][x]);
+                if (f32) m = round_diffused(m, cum_m[b][x]);
+                c.Mr[b][x] = m.real();
+                c.Mi[b][x] = m.imag();
+            }
+            const double n0 = std::norm(std::complex<double>(hs.Mr[b][0], hs.Mi[b][0]));
+            const double n1 = std::norm(std::complex<double>(hs.Mr[b][1], hs.Mi[b][1]));
+            c.piv[b] = -1;
+            c.br[b] = c.bi[b] = 0;
+            c.cp[b] = 1;
+            if (f32 && std::max(n0, n1) > 0) {
+                const int pv = n0 >= n1 ? 0 : 1;
+                const std::complex<double> w(hs.Mr[b][pv], hs.Mi[b][pv]), o(hs.Mr[b][1 - pv], hs.Mi[b][1 - pv]);
+                const std::complex<double> beta = round_diffused(o / w, cum_b[b]);
+                c.piv[b] = pv;
+                c.br[b] = beta.real();
+                c.bi[b] = beta.imag();
+                c.cp[b] = std::norm(w);
+            }
+        }
+        if ((size_t)k < E.args.size())
+            for (int b = 0; b < 2; b++)
+                for (int x = 0; x < 2; x++) {
+                    E.args[(size_t)k].Mr[b][x] = c.Mr[b][x];
+                    E.args[(size_t)k].Mi[b][x] = c.Mi[b][x];
+                }
+    }
+}
+
 static int make_args(Engine &E) {
     const HPlan &p = E.plan;
     E.args.resize((size_t)p.ns);
@@ -380,6 +473,7 @@ static int make_args(Engine &E) {
         a.m = s.m;
         E.args[(size_t)k] = a;
     }
+    apply_coeffs(E);
     size_t maxgrid = 1;
     E.lw.resize((size_t)p.ns);
     E.ln.resize((size_t)p.ns);
@@ -483,25 +577,17 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
             a.tau1[t] = hs.tau1[perm[s][t]] ^ swp[s];
             a.par[t] = hs.par[perm[s][t]];
         }
+        const Engine::Coef32 &cf = E.c32[(size_t)(gp.k0 + s)];
         for (int b = 0; b < 2; b++) {
-            for (int x = 0; x < 2; x++) { a.Mr[b][x] = hs.Mr[b][x]; a.Mi[b][x] = hs.Mi[b][x]; }
+            for (int x = 0; x < 2; x++) { a.Mr[b][x] = cf.Mr[b][x]; a.Mi[b][x] = cf.Mi[b][x]; }
             a.c[b] = hs.Mr[b][0] * hs.Mr[b][0] + hs.Mi[b][0] * hs.Mi[b][0] + hs.Mr[b][1] * hs.Mr[b][1] +
                      hs.Mi[b][1] * hs.Mi[b][1];
-            // factored form of a written complex64 step: pivot on the larger coefficient of the row
-            const double n0 = hs.Mr[b][0] * hs.Mr[b][0] + hs.Mi[b][0] * hs.Mi[b][0];
-            const double n1 = hs.Mr[b][1] * hs.Mr[b][1] + hs.Mi[b][1] * hs.Mi[b][1];
-            a.piv[b] = -1;
-            a.br[b] = a.bi[b] = 0;
-            a.cp[b] = 1;
-            if (E.prec == 64 && kinds[s] != GK_ANY && std::max(n0, n1) > 0) {
-                const int pv = n0 >= n1 ? 0 : 1;
-                const std::complex<double> w(hs.Mr[b][pv], hs.Mi[b][pv]), o(hs.Mr[b][1 - pv], hs.Mi[b][1 - pv]);
-                const std::complex<double> beta = o / w;
-                a.piv[b] = pv;
-                a.br[b] = beta.real();
-                a.bi[b] = beta.imag();
-                a.cp[b] = std::norm(w);
-            }
+            // factored form of a written complex64 step (FP32 arithmetic, compile-time shapes only)
+            const bool fact = kinds[s] != GK_ANY && cf.piv[b] >= 0;
+            a.piv[b] = fact ? cf.piv[b] : -1;
+            a.br[b] = fact ? cf.br[b] : 0;
+            a.bi[b] = fact ? cf.bi[b] : 0;
+            a.cp[b] = fact ? cf.cp[b] : 1;
         }
         for (int j = 0; j < g.nmem; j++) {
             for (int t = 0; t < g.ntq; t++) a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
@@ -621,7 +707,38 @@ static void build_sample_ops(Engine &E) {
 }
 
 // Chain-mode pass list: wide steps fused greedily into groups of up to fuse_depth steps.
+// The fused 'chain' passes of steps 0 .. hyb_K - 1 (groups do not cross hyb_K), for hybrid strings whose first
+// hyb_K steps are forced.
+static void build_hyb_ops(Engine &E) {
+    E.hyb_ops.clear();
+    const HPlan &p = E.plan;
+    for (int k = 0; k < E.hyb_K;) {
+        const HStep &hs = p.st[(size_t)k];
+        const int r = hs.nk + (hs.tqs.size() == 4 ? 2 : hs.tqs.size() == 2 ? 1 : 0);
+        bool done = false;
+        if (E.fuse_depth >= 2 && r >= GROUP_MIN_R) {
+            for (int d = std::min(std::min(E.fuse_depth, FUSE_MAX_STEPS), E.hyb_K - k); d >= 2 && !done; d--) {
+                GroupPlan gp;
+                if (!plan_group(p, k, d, 6, GROUP_MAX_L, gp)) continue;
+                Op op;
+                if (!fill_group(E, gp, op)) continue;
+                E.hyb_ops.push_back(op);
+                k += d;
+                done = true;
+            }
+        }
+        if (!done) {
+            Op op;
+            op.k0 = k;
+            op.d = 1;
+            E.hyb_ops.push_back(op);
+            k++;
+        }
+    }
+}
+
 static void build_chain_ops(Engine &E) {
+    build_hyb_ops(E);
     build_sample_ops(E);
     E.chain_ops.clear();
     if (!E.chain_shapes.empty() && ops_from_shapes(E, E.chain_shapes, E.chain_ops)) return;
@@ -988,6 +1105,9 @@ int gsb_hybrid(gsb_engine *e, const int8_t *forced, int64_t nstr, uint64_t seed,
     const int ns = E->plan.ns;
     int rc = check_bits(forced, nstr, ns, true);
     if (rc) return rc;
+    for (int64_t i = 0; i < nstr; i++)
+        for (int k = 0; k < E->hyb_K; k++)
+            if (forced[i * ns + k] < 0) return fail(GSB_E_PREFIX_FREE, "'?' before the forced prefix set by gsb_set_hybrid_prefix");
     std::vector<double> u((size_t)std::max<int64_t>(1, std::min<int64_t>(nstr, E->cap)) * (size_t)std::max(ns, 1));
     for (int64_t off = 0; off < nstr; off += E->cap) {
         const int64_t nb = std::min<int64_t>(E->cap, nstr - off);
@@ -1224,6 +1344,22 @@ int gsb_synchronize(gsb_engine *e) {
     return check_device(E);
 }
 
+int gsb_set_hybrid_prefix(gsb_engine *e, int K) {
+    if (!e) return fail(GSB_E_STATE, "null engine");
+    Engine *E = eng(e);
+    if (K < 0 || K > E->plan.ns) return fail(GSB_E_USAGE, "prefix length out of range");
+    DevGuard g(E->dev);
+    GSB_CK(cudaStreamSynchronize(E->stream));
+    E->hyb_K = K;
+    auto it = E->graphs.find(3);
+    if (it != E->graphs.end()) {
+        cudaGraphExecDestroy(it->second);
+        E->graphs.erase(it);
+    }
+    build_hyb_ops(*E);
+    return 0;
+}
+
 int gsb_set_guard(gsb_engine *e, gsb_engine *g, double log2_xmin) {
     if (!e) return fail(GSB_E_STATE, "null engine");
     Engine *E = eng(e);
@@ -1262,6 +1398,7 @@ int gsb_set_arith(gsb_engine *e, int bits) {
     E->arith = bits;
     for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);
     E->graphs.clear();
+    apply_coeffs(*E);
     for (int k = 0; k < E->plan.ns; k++) {
         E->lw[(size_t)k] = E->shape(E->args[(size_t)k], true);
         E->ln[(size_t)k] = E->shape(E->args[(size_t)k], false);
@@ -1609,6 +1746,7 @@ int gsb_set_matrices(gsb_engine *e, const double *M) {
                 s.Mi[b][x] = a.Mi[b][x] = im;
             }
     }
+    apply_coeffs(*E);
     for (auto &kv : E->graphs) cudaGraphExecDestroy(kv.second);   // the captured graphs hold M by value
     E->graphs.clear();
     build_chain_ops(*E);

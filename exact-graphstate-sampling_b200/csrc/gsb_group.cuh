@@ -1270,8 +1270,10 @@ __global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restr
             wj[s][0][x] = (T)(f * ga.st[s].Mi[bv][x]);
         }
     }
-    // complex64 arena: the factored coefficients of each written step (pivot, beta with the pass's scale, cp)
-    constexpr bool FACT = sizeof(E) == 8;
+    // complex64 arena with FP32 arithmetic: the factored coefficients of each written step (pivot, beta with the
+    // pass's scale, cp).  FP64 arithmetic (gsb_set_arith(64)) keeps the reference's complex64 arithmetic exactly:
+    // full rotation, direct branch norms, the store the only rounding.
+    constexpr bool FACT = sizeof(E) == 8 && std::is_same<T, float>::value;
     int fpiv[D];
     T fsc[D], fbr[D], fbi[D];
     double fcp[D];

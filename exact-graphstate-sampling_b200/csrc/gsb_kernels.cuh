@@ -618,6 +618,21 @@ __global__ void k_finish(DevState *st, double *logp_out, double *aux_out, int dr
 
 __global__ void k_set_item(DevState *st, int item) { st->item = item; }
 
+// Hybrid item whose first K steps are forced and ran as 'chain' passes (DRV_CHAIN1): from here on the run_steps
+// conventions (gsamp2.cpp:77-98).  The stored table is the true one times 2^-lsc, which is run_steps' logscale;
+// log2 Pr of the prefix is log2 |table|^2 + 2 lsc - K.  The forced bits of the prefix go to the output row.
+__global__ void k_hybrid_switch(DevState *st, const int8_t *forced, int8_t *bits_out, int ns, int K) {
+    const size_t row = (size_t)st->item * (size_t)ns;
+    for (int k = 0; k < K; k++) bits_out[row + k] = forced[row + k];
+    if (st->dead) {   // a zero-probability prefix: the chain epilogue zeroed every conditional from there on
+        for (int k = K; k < ns; k++) bits_out[row + k] = (int8_t)(forced[row + k] < 0 ? 0 : forced[row + k]);
+        st->logp = -INFINITY;
+        return;
+    }
+    st->logp = log2(st->prev) + 2.0 * st->lsc - K;
+    st->logscale = st->lsc;
+}
+
 // Live table at step K in logical (c, tq) order (the reference's prefix dump, gsamp2.cpp:170-174).
 template <typename E>
 __global__ void k_gather(const StepArgs s, const E *__restrict__ mem, int ntq, E *__restrict__ out) {

@@ -81,6 +81,7 @@ def _load():
                                     c.POINTER(c.c_int), c.POINTER(c.c_int)]),
         "gsb_test_withhold_tile_loads": (c.c_int, [P, c.c_int]),
         "gsb_set_guard": (c.c_int, [P, P, c.c_double]),
+        "gsb_set_hybrid_prefix": (c.c_int, [P, c.c_int]),
         "gsb_guard_evaluations": (c.c_int, [P, c.POINTER(c.c_int64)]),
         "gsb_autotune": (c.c_int, [P, c.c_int, c.c_int, c.POINTER(c.c_float), c.POINTER(c.c_float)]),
         "gsb_batch_open": (c.c_int, [c.POINTER(c.c_char_p), c.POINTER(c.c_size_t), c.c_int, c.c_int, c.c_int,
@@ -109,7 +110,7 @@ _lib = _load()
 EXPORTS = ("gsb_version", "gsb_last_error", "gsb_open_file", "gsb_open_text", "gsb_close", "gsb_info",
            "gsb_step_vertices", "gsb_prob", "gsb_chain", "gsb_sample", "gsb_sample_uniform", "gsb_hybrid",
            "gsb_dump_shape", "gsb_prefix", "gsb_resume", "gsb_chain_device", "gsb_sample_device",
-           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_probe_l2_copy", "gsb_test_withhold_tile_loads", "gsb_set_guard", "gsb_guard_evaluations", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
+           "gsb_synchronize", "gsb_set_stream", "gsb_set_arith", "gsb_set_matrices", "gsb_set_fusion", "gsb_fusion_groups", "gsb_sample_groups", "gsb_pass_list", "gsb_probe_l2_copy", "gsb_test_withhold_tile_loads", "gsb_set_guard", "gsb_guard_evaluations", "gsb_set_hybrid_prefix", "gsb_profile_steps", "gsb_launches_per_item", "gsb_validate_text",
            "gsb_cut_profile", "gsb_order_search", "gsb_dp_open_text", "gsb_dp_close", "gsb_dp_info", "gsb_dp_run",
            "gsb_dp_extend", "gsb_dp_extend_static", "gsb_grad_open_text", "gsb_grad_close", "gsb_grad_info",
            "gsb_grad_run", "gsb_autotune", "gsb_batch_open", "gsb_batch_close", "gsb_batch_set_strings", "gsb_batch_run",
@@ -151,11 +152,13 @@ def as_bits(strings, ns, allow_free=False):
     return a
 
 
-# Error model of the complex64 form (complex64 arena, FP32 arithmetic), measured against complex128 on the n = 70,
-# width-30 workload: the log2 Pr error of a string is close to normal with standard deviation
+# Error model of the complex64 form (complex64 arena, FP32 arithmetic), measured against complex128 on 2,048
+# uniform strings of the n = 70, width-30 workload: the log2 Pr error of a string is close to normal with mean 0
+# and standard deviation
 #     sigma(x) = C64_SIGMA_STEP * sqrt(nsteps) / sqrt(x),   x = Pr * 2^nsteps,
-# since the rounding of the stored table is absolute in units of its norm and each step adds its own.
-C64_SIGMA_STEP = 8.1e-8
+# since the rounding of the stored table is absolute in units of its norm and each step adds its own
+# (measured: sigma * sqrt(x) = 5.5e-7 at nsteps = 70).
+C64_SIGMA_STEP = 6.6e-8
 C64_GUARD_Z = 5.5
 
 
@@ -380,6 +383,10 @@ class Engine:
         complex128 Engine of the same plan (None detaches).  The guard must stay open while attached."""
         _check(_lib.gsb_set_guard(self.handle, None if guard is None else guard.handle, float(log2_xmin)))
         self._guard = guard          # keeps the guard alive as long as it is attached
+
+    def set_hybrid_prefix(self, K):
+        """hybrid() strings force their first K steps: those run as fused 'chain' passes (0 undoes it)."""
+        _check(_lib.gsb_set_hybrid_prefix(self.handle, int(K)))
 
     def guard_evaluations(self):
         n = ctypes.c_int64()

@@ -48,6 +48,9 @@ class HybridSampler:
         self.eng = gsb.Engine(first, precision=precision, device=device)
         self.slice_texts = [open(p).read() for p in self.slices]
         assert self.eng.ns == self.ns, "step_vertices does not match the plan"
+        if not self.slices:
+            # proposals force every step before the sampled suffix: those run as fused passes
+            self.eng.set_hybrid_prefix(self.ns - self.m_suffix)
 
     def to_step_string(self, bits, free_suffix):
         s = [0] * self.ns

@@ -150,6 +150,14 @@ int gsb_set_matrices(gsb_engine *e, const double *M);
  * Either way the stored table is complex64.  No effect on a complex128 engine. */
 int gsb_set_arith(gsb_engine *e, int bits);
 
+/* Hybrid strings whose first K steps are forced (no counterpart in the reference; K = 0, the default, undoes it).
+ * gsb_hybrid then runs those K steps as fused 'chain' passes, the way gsb_chain runs them, and the sampled steps
+ * K.. as the reference's run_steps does (gsamp2.cpp:77-98): the same bits, log2 Pr and conditionals, in about the
+ * time of one 'chain' string instead of one single-step sweep.  The hybrid driver's proposals have this form (first
+ * ND - m data steps drawn on the host, the last m sampled, doped_sampler.py:58-76).  A string with a '?' before
+ * step K is refused with GSB_E_PREFIX_FREE.  gsb_prefix and gsb_resume are unchanged. */
+int gsb_set_hybrid_prefix(gsb_engine *e, int K);
+
 /* Complex128 re-evaluation of unlikely strings (no counterpart in the reference).  A complex64 log2 Pr carries a
  * rounding error that grows like 1 / sqrt(x), x = Pr * 2^nsteps: the stored table's rounding is absolute in units
  * of its norm, and an unlikely string's amplitude is a small remainder of it.  With a complex128 engine `g` of the

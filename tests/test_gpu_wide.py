@@ -5,9 +5,10 @@ brute-force statevector at n = 24.
 
 Modes: "c128" (complex128 arena), "c64x" (complex64 arena, exact pair sums + FP64 rotation: the oracle's own
 complex64 arithmetic) and "c64" (complex64 arena, FP32 arithmetic, the default).  Tolerances: c128 |d log2 Pr| <=
-1e-9; c64x <= 1e-5; c64 <= 1e-5 x max(1, 2^(-n) / Pr): complex64 rounding is absolute in units of the table norm, so
-a string k times less likely than a typical one (Pr ~ 2^-n) carries k times the relative error.  Sampled bits are
-identical to the oracle's (same mt19937_64 streams).
+1e-9; c64x <= 1e-5; c64 within 6 standard deviations of the complex64 error model (gsb.c64_sigma: complex64
+rounding is absolute in units of the table norm, so the error grows as 1 / sqrt(Pr 2^n)), and the c64 form with its
+complex128 guard attached <= 1e-5 on every string.  Sampled bits are identical to the oracle's (same mt19937_64
+streams).
 """
 import os
 import tempfile
@@ -33,7 +34,8 @@ def lp_tol(mode, lp, n):
         return 1e-9
     if mode == "c64x":
         return 1e-5
-    return 1e-5 * max(1.0, 2.0 ** (-n - lp))
+    import gsb
+    return float(6 * gsb.c64_sigma(lp, n))
 
 
 def cond_tol(mode):
@@ -71,6 +73,19 @@ def test_wide_chain_prob_vs_oracle(wide_case, mode):
         olp = o.prob(strings[i])
         assert abs(lpp[i] - olp) <= lp_tol(mode, olp, n)
     o.close()
+    if mode == "c64":
+        # the complex64 form with its complex128 guard: 1e-5 of the complex128 oracle on every string
+        import gsb
+        o = Oracle(wide_case["path"], 128)
+        with engine(wide_case["path"], mode) as eng, gsb.Engine(wide_case["path"], precision=128) as e128:
+            eng.set_guard(e128, gsb.c64_guard_log2_xmin(ns))
+            lpg, _ = eng.chain(strings)
+            lpgp = eng.prob(strings[:6])
+        for i in range(len(strings)):
+            assert abs(lpg[i] - o.chain1(strings[i])[0]) <= 1e-5, i
+        for i in range(6):
+            assert abs(lpgp[i] - o.prob(strings[i])) <= 1e-5, i
+        o.close()
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -97,6 +112,19 @@ def test_wide_samples_and_hybrid_vs_oracle(wide_case, mode):
             assert list(hb[i]) == list(ob) and abs(hlp[i] - olp) <= lp_tol(mode, olp, n)
             if olp > -n - 3:
                 assert np.abs(hc[i] - oc).max() <= cond_tol(mode)
+        # the same lines with their forced prefix declared: fused passes for steps < ns - 6, the same results
+        eng.set_hybrid_prefix(ns - 6)
+        assert any(p[3] == 1 for p in eng.passes(0))   # the plan has fused chain passes
+        fb, flp, fc = eng.hybrid(lines, 11)
+        for i, ln in enumerate(lines):
+            ob, olp, oc = o.hybrid(ln, 11, i)
+            assert list(fb[i]) == list(ob) and abs(flp[i] - olp) <= lp_tol(mode, olp, n)
+            if olp > -n - 3:
+                assert np.abs(fc[i] - oc).max() <= cond_tol(mode)
+        with pytest.raises(gsb.GsbError) as e:
+            eng.hybrid([lines[0][:ns - 7] + "?" * 7], 11)
+        assert e.value.code == 8
+        eng.set_hybrid_prefix(0)
     o.close()
 
 
