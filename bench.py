@@ -82,7 +82,9 @@ def parse():
     ap.add_argument("--profile-mode", default="chain", choices=["chain", "sample"],
                     help="with --profile-chain: evaluate strings (chain) or draw exact samples (sample)")
     ap.add_argument("--profile-precision", type=int, default=64, choices=[64, 128])
-    ap.add_argument("--proposals", type=int, default=128, help="--form hybrid: proposals per timed run")
+    ap.add_argument("--proposals", type=int, default=64, help="--form hybrid: proposals per timed run")
+    ap.add_argument("--no-forms", dest="forms", action="store_false",
+                    help="headline line without the hybrid-driver and batched-launch sub-measurements")
     ap.add_argument("--form", default="headline", choices=["headline", "batch", "grad", "wide34", "hybrid"],
                     help="workload to measure (the default line is the headline n = 70, width-30 workload)")
     ap.add_argument("--batch-instances", type=int, default=512)
@@ -530,19 +532,31 @@ def run_gsb(args):
                                    "sample": "1 uniform random string of the workload, gsamp2 chain mode (complex64"
                                              + (f", -march=x86-64-{ref_isa(64)}" if kind == "reference" else "") + ")",
                                    "abs_dlog2p_vs_gpu_c128": abs(ref_lp - float(lp128[W * A])) if c128 else None}
+    if rank == 0 and world == 1 and args.forms:
+        # the hybrid driver and the batched launch on the same GPU, reported inside this line
+        out["forms"] = {}
+        for name, fn in (("hybrid", run_form_hybrid), ("batch", run_form_batch)):
+            try:
+                sub = argparse.Namespace(**vars(args))
+                sub.steps, sub.warmup = 5, 3
+                out["forms"][name] = fn(sub, emit=False)
+            except Exception as ex:   # a reported extra only
+                out["forms"][name] = {"unavailable": str(ex)[:200]}
     if rank == 0:
         print(json.dumps(out), flush=True)
     replicas.finish(world)
 
 
-def _form_line(form, metric, value, unit, hib, extra):
+def _form_line(form, metric, value, unit, hib, extra, emit=True):
     d = {"form": form, "metric": metric, "value": value, "unit": unit, "n_gpus": 1, "higher_is_better": hib,
          "data": "synthetic"}
     d.update(extra)
-    print(json.dumps(d), flush=True)
+    if emit:
+        print(json.dumps(d), flush=True)
+    return d
 
 
-def run_form_batch(args):
+def run_form_batch(args, emit=True):
     """Batched uneven workload: one persistent launch over all (instance, prefix) items."""
     import numpy as np
     import gsb
@@ -583,7 +597,17 @@ def run_form_batch(args):
         byt += 16 * E * (pre + 4 * suf + 2 * snap + 3 * 2 * snap)
     peak, kind = peaks()
     l2 = max(gsb.probe_l2_copy(mib=mib) for mib in (16, 24, 32))
-    _form_line("batch", "amps/s, 512 instances n in [16,40] x 64 strings, one persistent launch", nstr / (ms / 1e3),
+    # working set of the items in flight: each CTA team holds one wide item's arena and snapshot (2 x 2^R x E)
+    wide = [1 << r for r in widths if r > small_R] or [0]
+    working_set = min(len(wide), per_sm * 148) * 2 * E * float(np.mean(wide))
+    l2_bytes = 126e6
+    roof_l2 = {"bound": "l2", "achieved": byt / (ms / 1e3) / 1e9, "peak": l2, "unit": "GB/s",
+               "frac": byt / (ms / 1e3) / 1e9 / l2,
+               "peak_kind": "measured here: L2 copy bandwidth (gsb_probe_l2_copy, best of 16/24/32 MiB buffers, one "
+                            "launch of 400 passes)"}
+    roof_hbm = {"bound": "hbm", "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_kind": kind}
+    return _form_line("batch", "amps/s, 512 instances n in [16,40] x 64 strings, one persistent launch", nstr / (ms / 1e3),
                "amps/s", True, {
                    "ms_per_launch": ms, "strings": int(nstr), "instances": len(plans),
                    "widths": {"min": int(min(widths)), "max": int(max(widths)), "mean": float(np.mean(widths))},
@@ -591,17 +615,14 @@ def run_form_batch(args):
                                                                                  "ctas_per_sm": per_sm},
                    "c128": {"ms_per_launch": ms128, "max_abs_dlog2p_c64_vs_c128": float(d.max()),
                             "median_abs_dlog2p": float(np.median(d))},
-                   "roofline": {"bound": "l2", "achieved": byt / (ms / 1e3) / 1e9, "peak": l2, "unit": "GB/s",
-                                "frac": byt / (ms / 1e3) / 1e9 / l2,
-                                "peak_kind": "measured here: L2 copy bandwidth (gsb_probe_l2_copy, best of "
-                                             "16/24/32 MiB buffers, one launch of 400 passes)",
-                                "note": "team tables of <= 2^20 entries, each reused through an item's prefix and "
-                                        "suffix sweeps: the launch reads and writes them mostly in L2"},
-                   "roofline_hbm": {"bound": "hbm", "achieved": byt / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                                    "frac": byt / (ms / 1e3) / 1e9 / peak, "peak_kind": kind},
+                   "roofline": roof_l2 if working_set <= l2_bytes else roof_hbm,
+                   "roofline_other": roof_hbm if working_set <= l2_bytes else roof_l2,
+                   "working_set_bytes": working_set,
+                   "roofline_choice": "the L2 line when the wide items in flight (one per CTA team: arena and "
+                                      "snapshot) fit the 126 MB L2, else the HBM line",
                    "orders": args.batch_order,
                    "host_planning_s": t_plan, "steps": args.steps, "warmup": args.warmup,
-               })
+               }, emit=emit)
 
 
 def run_form_grad(args):
@@ -714,11 +735,12 @@ def run_form_wide34(args):
                               "max_abs_dlog2p": max(abs(a - b) for a, b in check), "seconds": t_check}})
 
 
-def run_form_hybrid(args):
+def run_form_hybrid(args, emit=True):
     """Hybrid rejection sampling of the headline instance in process (hybrid_sampler, the reference's doped_sampler
     driver with the executor kept loaded): proposals draw the first 70 - m step bits uniformly and sample the last
-    m = 16 exactly.  Seconds per proposal with the proposals batched into gsb_hybrid calls, and with one call per
-    proposal (the reference's structure without its process start-up)."""
+    m = 16 exactly.  Seconds per proposal as the driver runs them (forced prefix in fused passes, 64 proposals per
+    gsb_hybrid call), with one call per proposal, and with every step a single-step pass (no declared prefix: the
+    structure of the reference's executor, without its process start-up)."""
     import gsb
     import hybrid_sampler
     import workloads
@@ -729,10 +751,12 @@ def run_form_hybrid(args):
         sv = os.path.join(td, "sv.json")
         json.dump([s["v"] for s in w["steps"]], open(sv, "w"))
         hs = hybrid_sampler.HybridSampler(plan, sv, na=0, nd=70, m=16, precision=64)
-        hs.sample(4, 1, 2.0, os.path.join(td, "warm.txt"))
         res = {}
-        for name, batch in (("batched", 64), ("one_call_per_proposal", 1)):
+        K = hs.ns - hs.m_suffix
+        for name, batch, prefix in (("batched", 64, K), ("one_call_per_proposal", 1, K), ("unfused_steps", 64, 0)):
             hs.BATCH = batch
+            hs.eng.set_hybrid_prefix(prefix)
+            hs.sample(2, 3, 2.0, os.path.join(td, f"warm_{name}.txt"))
             gsb.Engine.synchronize(hs.eng)
             t0 = time.perf_counter()
             acc, zmax = hs.sample(args.proposals, 7, 2.0, os.path.join(td, f"{name}.txt"))
@@ -740,18 +764,22 @@ def run_form_hybrid(args):
             res[name] = (time.perf_counter() - t0) / args.proposals
         same = open(os.path.join(td, "batched.txt")).read().split("\n")
         one = open(os.path.join(td, "one_call_per_proposal.txt")).read().split("\n")
+        unf = open(os.path.join(td, "unfused_steps.txt")).read().split("\n")
         import re
 
         def strip(ls):   # the lines without their wall-time fields
             return [" ".join(t for t in ln.split() if not re.fullmatch(r"[0-9.]+s", t)) for ln in ls]
         hs.close()
-    _form_line("hybrid", "s/proposal (hybrid rejection sampling, n=70 w=30, m=16, complex64)", res["batched"],
+    return _form_line("hybrid", "s/proposal (hybrid rejection sampling, n=70 w=30, m=16, complex64)", res["batched"],
                "s/proposal", False,
                {"config": {"workload": WORKLOAD, "proposals": args.proposals, "m_suffix": 16, "cap": 2.0},
                 "one_call_per_proposal_s": res["one_call_per_proposal"],
-                "batched_over_single": res["one_call_per_proposal"] / res["batched"],
-                "same_decisions_and_bits": strip(same) == strip(one),
-                "accepted": acc, "max_z": zmax})
+                "unfused_steps_s": res["unfused_steps"],
+                "speedup_over_unfused": res["unfused_steps"] / res["batched"],
+                "same_lines_all_three": strip(same) == strip(one),
+                "same_decisions_unfused": [ln.split()[:2] for ln in strip(same) if ln and not ln.startswith("#")] ==
+                                          [ln.split()[:2] for ln in strip(unf) if ln and not ln.startswith("#")],
+                "accepted": acc, "max_z": zmax}, emit=emit)
 
 
 if __name__ == "__main__":

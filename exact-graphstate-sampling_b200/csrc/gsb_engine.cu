@@ -17,6 +17,7 @@
 #include <map>
 #include <random>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "gsb.h"
@@ -109,11 +110,17 @@ static void *pick_group(int d, int tr) {
     if (tr) return d == 2 ? (void *)k_group<E, T, 2, 1> : (void *)k_group<E, T, 1, 1>;
     return d == 3 ? (void *)k_group<E, T, 3, 0> : (void *)k_group<E, T, 2, 0>;
 }
+// the three-CTAs-per-SM instantiations (complex64, FP32 arithmetic)
+static void *pick_group3(int d, int tr) {
+    if (tr) return d == 2 ? (void *)k_group<float2, float, 2, 1, 3> : (void *)k_group<float2, float, 1, 1, 3>;
+    return d == 3 ? (void *)k_group<float2, float, 3, 0, 3> : (void *)k_group<float2, float, 2, 0, 3>;
+}
 
 // One pass of an item: a single step (group == false: norm pass + write pass when sampling) or a fused group that
 // writes d steps and, with tr = 1, evaluates the next step's branch norms (sampling only).
 struct Op {
     int k0 = 0, d = 1, tr = 0, lcap = 0;   // lcap: the tile-size cap the pass was built with (fused passes)
+    int minb = 2;                          // CTAs per SM the fused kernel is built for (2, or 3: pick_group3)
     bool group = false;
     bool norm_first = false;  // sampling: a norm pass of step k0 runs first (its bit has no other source)
     GroupArgs ga;
@@ -137,9 +144,10 @@ constexpr int GROUP_MIN_R = 12;                     // steps below 2^12 entries 
 
 // What a pass is, without its arguments: rebuilt with the current matrices whenever they change.
 struct OpShape {
-    int k0 = 0, d = 1, tr = 0, lcap = 0, src = 0;
+    int k0 = 0, d = 1, tr = 0, lcap = 0, src = 0, minb = 2;
     bool group = false, norm_first = false;
 };
+constexpr uint32_t GROUP_SMEM_3 = 72 * 1024;        // shared memory of a fused-pass CTA when three share an SM
 
 template <typename E, typename T>
 static uint32_t group_smem_bytes(int D, int TR, const int (&ssz)[4], int L) {
@@ -380,8 +388,9 @@ struct Engine {
 // Float rounding of the FP32 kernels' coefficients by error diffusion.  A rounded coefficient c' = c (1 + d)
 // scales every amplitude path through it; the real part of d biases log2 Pr, the same way for every string, and
 // with round-to-nearest a plan whose steps repeat one matrix (a circuit with one rotation on every qubit) adds
-// those biases up step after step.  Each value is therefore rounded up or down (either is within one ulp) so that
-// the running sum of Re d over the steps, per coefficient role, stays within about one ulp of zero.
+// those biases up step after step.  Each occurrence of a value is therefore rounded up or down (either is within
+// one ulp) so that the running sum of Re d over that value's occurrences stays within about one ulp of zero; the
+// first occurrence rounds to nearest, so a plan of distinct matrices keeps round-to-nearest throughout.
 static std::complex<double> round_diffused(std::complex<double> v, double &cum) {
     if (v == 0.0) return v;
     auto pair = [](double x, float &lo, float &hi) {
@@ -414,14 +423,25 @@ static void apply_coeffs(Engine &E) {
     const HPlan &p = E.plan;
     const bool f32 = E.prec == 64 && E.arith == 32;
     E.c32.assign((size_t)p.ns, Engine::Coef32());
-    double cum_m[2][2] = {{0, 0}, {0, 0}}, cum_b[2] = {0, 0};
+    // running sums of Re d per (role, exact value): roles 0-3 the M entries [b][x], 4-5 the ratios of bit b
+    std::map<std::tuple<int, double, double>, double> cum;
+    auto rnd = [&](int role, std::complex<double> v) {
+        auto key = std::make_tuple(role, v.real(), v.imag());
+        auto it = cum.find(key);
+        if (it == cum.end()) {   // first occurrence: round to nearest
+            const std::complex<double> c((double)(float)v.real(), (double)(float)v.imag());
+            cum[key] = v == 0.0 ? 0.0 : ((c - v) / v).real();
+            return c;
+        }
+        return round_diffused(v, it->second);
+    };
     for (int k = 0; k < p.ns; k++) {
         const HStep &hs = p.st[(size_t)k];
         Engine::Coef32 &c = E.c32[(size_t)k];
         for (int b = 0; b < 2; b++) {
             for (int x = 0; x < 2; x++) {
                 std::complex<double> m(hs.Mr[b][x], hs.Mi[b][x]);
-                if (f32) m = round_diffused(m, cum_m[b][x]);
+                if (f32) m = rnd(2 * b + x, m);
                 c.Mr[b][x] = m.real();
                 c.Mi[b][x] = m.imag();
             }
@@ -433,7 +453,7 @@ static void apply_coeffs(Engine &E) {
             if (f32 && std::max(n0, n1) > 0) {
                 const int pv = n0 >= n1 ? 0 : 1;
                 const std::complex<double> w(hs.Mr[b][pv], hs.Mi[b][pv]), o(hs.Mr[b][1 - pv], hs.Mi[b][1 - pv]);
-                const std::complex<double> beta = round_diffused(o / w, cum_b[b]);
+                const std::complex<double> beta = rnd(4 + b, o / w);
                 c.piv[b] = pv;
                 c.br[b] = beta.real();
                 c.bi[b] = beta.imag();
@@ -443,8 +463,8 @@ static void apply_coeffs(Engine &E) {
         if ((size_t)k < E.args.size())
             for (int b = 0; b < 2; b++)
                 for (int x = 0; x < 2; x++) {
-                    E.args[(size_t)k].Mr[b][x] = c.Mr[b][x];
-                    E.args[(size_t)k].Mi[b][x] = c.Mi[b][x];
+                    E.args[(size_t)k].Mr32[b][x] = c.Mr[b][x];
+                    E.args[(size_t)k].Mi32[b][x] = c.Mi[b][x];
                 }
     }
 }
@@ -495,10 +515,11 @@ static bool analytic_step(const HStep &hs) {
 
 // Group arguments of a fused pass from the host derivation and the steps' descriptors.  The pass writes stage gp.ws;
 // with gp.ws = gp.d - 1 the last step is the trailing norm step.
-static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_MAX_L) {
+static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_MAX_L, int minb = 2) {
     const HPlan &p = E.plan;
     const int D = gp.ws, TR = gp.d - gp.ws;
     if (gp.stage_size[0] > 32 || gp.stage_size[D] > 32) return false;
+    if (minb != 2 && (minb != 3 || E.prec != 64 || E.arith != 32)) return false;
     // tile size: the largest 2^L classes whose pipeline buffers fit the budget (6 <= L: a warp needs 32 class pairs)
     auto smem_at = [&](int L) -> uint32_t {
         const int ssz[4] = {gp.stage_size[0], gp.stage_size[1], gp.stage_size[2], gp.stage_size[3]};
@@ -507,8 +528,9 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
         return group_smem_bytes<float2, float>(D, TR, ssz, L);
     };
     int L = std::min(gp.L, std::min(lcap, GROUP_MAX_L));
-    while (L > 6 && smem_at(L) > GROUP_SMEM_PREF) L--;
-    if (smem_at(L) > GROUP_SMEM_BUDGET || L < 6) return false;
+    const uint32_t pref = minb == 3 ? GROUP_SMEM_3 : GROUP_SMEM_PREF, budget = minb == 3 ? GROUP_SMEM_3 : GROUP_SMEM_BUDGET;
+    while (L > 6 && smem_at(L) > pref) L--;
+    if (smem_at(L) > budget || L < 6) return false;
     GroupArgs &ga = op.ga;
     memset(&ga, 0, sizeof ga);
     ga.d = gp.d;
@@ -600,11 +622,12 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
     op.d = gp.ws;
     op.tr = gp.d - gp.ws;
     op.lcap = lcap;
+    op.minb = minb;
     op.smem = smem_at(L);
     op.ntiles = 1u << ga.nbhi;
     if (E.prec == 128) op.fn = pick_group<double2, double>(op.d, op.tr);
     else if (E.arith == 64) op.fn = pick_group<float2, double>(op.d, op.tr);
-    else op.fn = pick_group<float2, float>(op.d, op.tr);
+    else op.fn = minb == 3 ? pick_group3(op.d, op.tr) : pick_group<float2, float>(op.d, op.tr);
     if (cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET) != cudaSuccess)
         return false;
     int nb = 0;
@@ -630,7 +653,8 @@ static bool make_op(Engine &E, const OpShape &sh, Op &op) {
         return true;
     }
     GroupPlan gp;
-    if (!plan_group(E.plan, sh.k0, sh.d + sh.tr, 6, sh.lcap, gp, sh.d) || !fill_group(E, gp, op, sh.lcap)) return false;
+    if (!plan_group(E.plan, sh.k0, sh.d + sh.tr, 6, sh.lcap, gp, sh.d) || !fill_group(E, gp, op, sh.lcap, sh.minb))
+        return false;
     op.norm_first = sh.norm_first;
     op.ga.src = sh.src;
     return true;
@@ -1488,14 +1512,17 @@ static int autotune(Engine &E, int mode, int reps) {
     }
     // fused candidates starting at k, with their times (distinct tile sizes only)
     auto fused = [&](int k, int d, int tr, std::vector<std::pair<OpShape, double>> &out) -> int {
-        int lastL = -1;
-        for (int lcap : {GROUP_MAX_L, GROUP_MAX_L - 1, GROUP_MAX_L - 2}) {
+        for (int minb : {2, 3}) {
+          if (minb == 3 && (E.prec != 64 || E.arith != 32)) continue;
+          int lastL = -1;
+          for (int lcap : {GROUP_MAX_L, GROUP_MAX_L - 1, GROUP_MAX_L - 2}) {
             OpShape sh;
             sh.group = true;
             sh.k0 = k;
             sh.d = d;
             sh.tr = tr;
             sh.lcap = lcap;
+            sh.minb = minb;
             sh.src = GSRC_NORM;   // timing: the bit of step k as a norm pass would leave it
             Op op;
             if (!make_op(E, sh, op) || op.ga.L == lastL) continue;
@@ -1503,6 +1530,7 @@ static int autotune(Engine &E, int mode, int reps) {
             const double t = timer([&] { return E.launch_op(op, drv, true, false); });
             if (t < 0) return fail(GSB_E_CUDA, "autotuner: a timing launch failed");
             out.push_back({sh, t});
+          }
         }
         return 0;
     };

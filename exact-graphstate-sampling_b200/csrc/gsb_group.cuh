@@ -186,6 +186,22 @@ __device__ __forceinline__ void st_perm(double2 *m, uint32_t pos, const double (
 #pragma unroll
     for (int c = 0; c < P; c++) m[pos ^ (uint32_t)c] = make_double2(r[c], i[c]);
 }
+// A class pair (even p, then p + 1) of a complex64 block as one aligned 16-byte access: the pair's two entries sit at
+// pos and pos ^ 1 (pos = p ^ offset bits), i.e. in the 16 bytes at pos & ~1, swapped when bit 0 of the offset is set
+// (uniform across a warp).  One access instead of two 8-byte ones at a 16-byte thread stride, which take twice the
+// shared-memory wavefronts.
+__device__ __forceinline__ void ld_pair16(const float2 *m, uint32_t pos, float (&r)[2], float (&i)[2]) {
+    const float4 v = *reinterpret_cast<const float4 *>(m + (pos & ~1u));
+    const bool sw = (pos & 1u) != 0;
+    r[0] = sw ? v.z : v.x; i[0] = sw ? v.w : v.y;
+    r[1] = sw ? v.x : v.z; i[1] = sw ? v.y : v.w;
+}
+__device__ __forceinline__ void st_pair16(float2 *m, uint32_t pos, const float (&r)[2], const float (&i)[2]) {
+    float4 *q = reinterpret_cast<float4 *>(m + (pos & ~1u));
+    if (pos & 1u) *q = make_float4(r[1], i[1], r[0], i[0]);   // a warp-uniform choice: one predicated store
+    else *q = make_float4(r[0], i[0], r[1], i[1]);
+}
+
 // shared memory [index][class]: P consecutive values
 template <int P>
 __device__ __forceinline__ void lds_cls(const float2 *q, float (&r)[P], float (&i)[P]) {
@@ -652,8 +668,14 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
 #pragma unroll
             for (int t = 0; t < NTQ; t++) {
                 T vr[P], vi[P];
-                if (FIRST) ld_perm<P>(reinterpret_cast<const E *>(smem + in) + ib[t], pc ^ zl[t], vr, vi);
-                else lds_cls<P>(reinterpret_cast<const V *>(smem + in) + (ib[t] + pc), vr, vi);
+                if (FIRST) {
+                    if constexpr (P == 2 && std::is_same<T, float>::value)
+                        ld_pair16(reinterpret_cast<const float2 *>(smem + in) + ib[t], pc ^ zl[t], vr, vi);
+                    else
+                        ld_perm<P>(reinterpret_cast<const E *>(smem + in) + ib[t], pc ^ zl[t], vr, vi);
+                } else {
+                    lds_cls<P>(reinterpret_cast<const V *>(smem + in) + (ib[t] + pc), vr, vi);
+                }
                 const int op = S::pout(t), oq = S::qout(t);
                 const bool p_first = S::first_p(op) == t, q_first = S::first_q(oq) == t;
 #pragma unroll
@@ -697,7 +719,12 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
                     nsum = fmaT(re, re, nsum);
                     nsum = fmaT(im, im, nsum);
                 }
-                if (LAST) st_perm<P>(ob[tau], pc ^ ol[tau], orr, oii);
+                if (LAST) {
+                    if constexpr (P == 2 && std::is_same<T, float>::value)
+                        st_pair16(reinterpret_cast<float2 *>(ob[tau]), pc ^ ol[tau], orr, oii);
+                    else
+                        st_perm<P>(ob[tau], pc ^ ol[tau], orr, oii);
+                }
                 if (STS) sts_cls<P>(reinterpret_cast<V *>(smem + out) + (oidx[tau] + pc), orr, oii);
             }
         }
@@ -773,11 +800,10 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
             for (int t = 0; t < NTQ; t++) {
                 f32x2 VR, VI;
                 if (FIRST) {
-                    const float2 *src = reinterpret_cast<const float2 *>(smem + in) + ib[t];
-                    const uint32_t pos = pc ^ zl[t];
-                    const float2 a = src[pos], b = src[pos ^ 1u];
-                    VR = f2_pack(a.x, b.x);
-                    VI = f2_pack(a.y, b.y);
+                    float r2[2], i2[2];
+                    ld_pair16(reinterpret_cast<const float2 *>(smem + in) + ib[t], pc ^ zl[t], r2, i2);
+                    VR = f2_pack(r2[0], r2[1]);
+                    VI = f2_pack(i2[0], i2[1]);
                 } else {
                     const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib[t] + pc));
                     VR = f2_pack(v.x, v.y);
@@ -820,9 +846,8 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
                     f2_unpack(RE, r0, r1);
                     f2_unpack(IM, i0, i1);
                     if (LAST) {
-                        const uint32_t pos = pc ^ ol[tau];
-                        ob[tau][pos] = make_float2(r0, i0);
-                        ob[tau][pos ^ 1u] = make_float2(r1, i1);
+                        const float rr2[2] = {r0, r1}, ii2[2] = {i0, i1};
+                        st_pair16(ob[tau], pc ^ ol[tau], rr2, ii2);
                     }
                     if (STS)
                         *reinterpret_cast<float4 *>(reinterpret_cast<float2 *>(smem + out) + (oidx[tau] + pc)) =
@@ -1226,10 +1251,11 @@ __host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L) {
 // buffer n & 1 (completion on that buffer's mbarrier) two tiles ahead: the loads of tile n + 2 are issued as soon as
 // tile n's first step has read its buffer.  The last written step stores straight to the arena.  A tile's writes
 // never reach another class's input (checked on the host), so the early loads are race-free.
-// Two CTAs per SM (the shared-memory budget allows no more), so up to 128 registers a thread: without this bound the
-// compiler kept some instantiations at 64-80 registers and spilled.
-template <typename E, typename T, int D, int TR>
-__global__ void __launch_bounds__(256, 2) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
+// MINB CTAs per SM: 2 by default (up to 128 registers a thread: without this bound the compiler kept some
+// instantiations at 64-80 registers and spilled); 3 for complex64 FP32 passes with tiles small enough for three
+// CTAs' shared memory (85 registers: more resident warps to hide the dependent arithmetic), an autotuner candidate.
+template <typename E, typename T, int D, int TR, int MINB = 2>
+__global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
     DevState *st = cx.st;
     if (*(volatile int *)&st->dead) return;
     extern __shared__ __align__(16) unsigned char smem[];

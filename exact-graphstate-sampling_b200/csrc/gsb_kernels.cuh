@@ -388,8 +388,10 @@ __global__ void __launch_bounds__(256) k_pair64(const StepArgs s, float2 *__rest
         for (int x = 0; x < 2; x++) {
             const int bb = WRITE ? P.bv : b;
             const double f = WRITE ? P.sc : 1.0;
-            wr[b][x] = (T)(f * s.Mr[bb][x]);
-            wi[b][x] = (T)(f * s.Mi[bb][x]);
+            // FP32 arithmetic takes the engine's float-rounded coefficients; FP64 the plan's own
+            const bool f32 = sizeof(T) == 4;
+            wr[b][x] = (T)(f * (f32 ? s.Mr32[bb][x] : s.Mr[bb][x]));
+            wi[b][x] = (T)(f * (f32 ? s.Mi32[bb][x] : s.Mi[bb][x]));
         }
     uint64_t Tt = 0;
     for (int j = 0; j < 8; j++)

@@ -10,6 +10,7 @@ struct StepArgs {
     uint64_t tq[4];         // distinct coset offsets, ascending
     uint64_t g, rhoc;
     double Mr[2][2], Mi[2][2];
+    double Mr32[2][2], Mi32[2][2];   // the same rounded to float values for the FP32 kernels (the engine's apply_coeffs)
     int nk, k, ntq, m;
     int tau0[4], tau1[4], par[4];
 };
