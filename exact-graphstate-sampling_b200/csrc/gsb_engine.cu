@@ -150,8 +150,8 @@ struct OpShape {
 constexpr uint32_t GROUP_SMEM_3 = 72 * 1024;        // shared memory of a fused-pass CTA when three share an SM
 
 template <typename E, typename T>
-static uint32_t group_smem_bytes(int D, int TR, const int (&ssz)[4], int L) {
-    if (TR) return D == 2 ? group_smem<E, T, 2, 1>(ssz, L).total : group_smem<E, T, 1, 1>(ssz, L).total;
+static uint32_t group_smem_bytes(int D, int TR, const int (&ssz)[4], int L, bool fold = false) {
+    if (TR) return D == 2 ? group_smem<E, T, 2, 1>(ssz, L, fold).total : group_smem<E, T, 1, 1>(ssz, L).total;
     return D == 3 ? group_smem<E, T, 3, 0>(ssz, L).total : group_smem<E, T, 2, 0>(ssz, L).total;
 }
 
@@ -520,28 +520,6 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
     const int D = gp.ws, TR = gp.d - gp.ws;
     if (gp.stage_size[0] > 32 || gp.stage_size[D] > 32) return false;
     if (minb != 2 && (minb != 3 || E.prec != 64 || E.arith != 32)) return false;
-    // tile size: the largest 2^L classes whose pipeline buffers fit the budget (6 <= L: a warp needs 32 class pairs)
-    auto smem_at = [&](int L) -> uint32_t {
-        const int ssz[4] = {gp.stage_size[0], gp.stage_size[1], gp.stage_size[2], gp.stage_size[3]};
-        if (E.prec == 128) return group_smem_bytes<double2, double>(D, TR, ssz, L);
-        if (E.arith == 64) return group_smem_bytes<float2, double>(D, TR, ssz, L);
-        return group_smem_bytes<float2, float>(D, TR, ssz, L);
-    };
-    int L = std::min(gp.L, std::min(lcap, GROUP_MAX_L));
-    const uint32_t pref = minb == 3 ? GROUP_SMEM_3 : GROUP_SMEM_PREF, budget = minb == 3 ? GROUP_SMEM_3 : GROUP_SMEM_BUDGET;
-    while (L > 6 && smem_at(L) > pref) L--;
-    if (smem_at(L) > budget || L < 6) return false;
-    GroupArgs &ga = op.ga;
-    memset(&ga, 0, sizeof ga);
-    ga.d = gp.d;
-    ga.L = L;
-    std::vector<uint64_t> bhi;
-    for (int j = L; j < gp.L; j++) bhi.push_back(1ULL << j);    // low unit vectors beyond the tile
-    bhi.insert(bhi.end(), gp.bhi.begin(), gp.bhi.end());
-    if (bhi.size() > 30) return false;                           // tile index fits 32 bits with room
-    ga.nbhi = (int)bhi.size();
-    for (size_t j = 0; j < bhi.size(); j++) ga.bhi[j] = bhi[j];
-    for (int s = 0; s <= gp.d; s++) ga.ssz[s] = gp.stage_size[s];
     // Canonical offset order per step (the kernel's compile-time dataflow shapes, GK_*): for m = 2 with every x = 1
     // term in the other output than its offset's x = 0 term, offsets whose x = 0 term goes to output 0 come first,
     // and the outputs are relabelled when more than half go to output 1.  Other steps keep their order (GK_ANY).
@@ -574,6 +552,54 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
             if (swp[s]) std::swap(cs[s].out_idx[j][0], cs[s].out_idx[j][1]);
         }
     }
+    // Folded sampling pass (GroupArgs::fold): two written steps whose second is a one-offset growth step of the
+    // factored complex64 form for both bits, then a shaped trailing step.  The trailing step then reads stage 1
+    // through the growth step's map, and the written stage needs no shared memory.
+    bool fold = false;
+    if (E.prec == 64 && E.arith == 32 && minb == 2 && D == 2 && TR == 1 && kinds[1] == GK_1_0 && kinds[2] != GK_ANY) {
+        const Engine::Coef32 &cg = E.c32[(size_t)(gp.k0 + 1)];
+        fold = cg.piv[0] >= 0 && cg.piv[1] >= 0;
+    }
+    // trailing member j, offset t reads written-stage index i = in_idx[j][t]: the growth step's member m with
+    // out_idx[m][tau] = i, whose input is stage-1 index in_idx[m][0]
+    unsigned char fsrc[16][4] = {}, ftau[16][4] = {}, fmem[16][4] = {};
+    if (fold) {
+        const GroupPlan::Step &g1 = cs[1], &g2 = cs[2];
+        for (int j2 = 0; j2 < g2.nmem && fold; j2++)
+            for (int t = 0; t < g2.ntq && fold; t++) {
+                const int i2 = g2.in_idx[j2][t];
+                int found = -1, tau_f = 0;
+                for (int m = 0; m < g1.nmem && found < 0; m++)
+                    for (int tau = 0; tau < 2; tau++)
+                        if (g1.out_idx[m][tau] == i2) { found = m; tau_f = tau; break; }
+                if (found < 0) { fold = false; break; }   // not a value the growth step writes: leave it unfolded
+                fsrc[j2][t] = (unsigned char)g1.in_idx[found][0];
+                ftau[j2][t] = (unsigned char)tau_f;
+                fmem[j2][t] = (unsigned char)found;
+            }
+    }
+    // tile size: the largest 2^L classes whose pipeline buffers fit the budget (6 <= L: a warp needs 32 class pairs)
+    auto smem_at = [&](int L) -> uint32_t {
+        const int ssz[4] = {gp.stage_size[0], gp.stage_size[1], gp.stage_size[2], gp.stage_size[3]};
+        if (E.prec == 128) return group_smem_bytes<double2, double>(D, TR, ssz, L);
+        if (E.arith == 64) return group_smem_bytes<float2, double>(D, TR, ssz, L);
+        return group_smem_bytes<float2, float>(D, TR, ssz, L, fold);
+    };
+    int L = std::min(gp.L, std::min(lcap, GROUP_MAX_L));
+    const uint32_t pref = minb == 3 ? GROUP_SMEM_3 : GROUP_SMEM_PREF, budget = minb == 3 ? GROUP_SMEM_3 : GROUP_SMEM_BUDGET;
+    while (L > 6 && smem_at(L) > pref) L--;
+    if (smem_at(L) > budget || L < 6) return false;
+    GroupArgs &ga = op.ga;
+    memset(&ga, 0, sizeof ga);
+    ga.d = gp.d;
+    ga.L = L;
+    std::vector<uint64_t> bhi;
+    for (int j = L; j < gp.L; j++) bhi.push_back(1ULL << j);    // low unit vectors beyond the tile
+    bhi.insert(bhi.end(), gp.bhi.begin(), gp.bhi.end());
+    if (bhi.size() > 30) return false;                           // tile index fits 32 bits with room
+    ga.nbhi = (int)bhi.size();
+    for (size_t j = 0; j < bhi.size(); j++) ga.bhi[j] = bhi[j];
+    for (int s = 0; s <= gp.d; s++) ga.ssz[s] = gp.stage_size[s];
     {
         const GroupPlan::Step &g0 = cs[0], &gd = cs[gp.ws - 1];
         const uint64_t mask = (1ULL << L) - 1;
@@ -616,6 +642,12 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
             for (int tau = 0; tau < g.m; tau++) a.out_idx[j][tau] = (unsigned char)g.out_idx[j][tau];
             a.mpar[j] = (unsigned char)g.mpar[j];
         }
+    }
+    if (fold) {
+        ga.fold = 1;
+        memcpy(ga.fsrc, fsrc, sizeof fsrc);
+        memcpy(ga.ftau, ftau, sizeof ftau);
+        memcpy(ga.fmem, fmem, sizeof fmem);
     }
     op.group = true;
     op.k0 = gp.k0;

@@ -45,6 +45,12 @@ struct GroupArgs {
     uint64_t blk_out[32];  // written-stage offsets, bits >= L: output block i goes to the arena block at TB ^ blk_out[i]
     uint32_t z0lo[16][4];  // first step: member j, offset t -> bits < L of its stage-0 offset (position p ^ z0lo)
     uint32_t zdlo[16][2];  // last written step: member j, output tau -> bits < L of its offset
+    // fold = 1 (complex64 sampling passes of two written steps whose second is a one-offset growth step, GK_1_0): the
+    // second step's outputs are not kept in shared memory; the trailing step reads the stage before it and applies
+    // that step's map per term: its member j, offset t reads stage-1 value fsrc[j][t], output ftau[j][t] of the
+    // growth step's member fmem[j][t]
+    int fold;
+    unsigned char fsrc[16][4], ftau[16][4], fmem[16][4];
     GroupStepArgs st[3];
 };
 
@@ -1043,6 +1049,120 @@ __device__ __forceinline__ void group_trail_abc_pk(const GroupArgs &ga, const Gr
     f2_unpack(CI, a, b); acc[3] += a + b;
 }
 
+// The shared-sum trailing step of a folded pass (GroupArgs::fold, packed FP32): the written stage is the output of a
+// one-offset growth step g (GK_1_0) applied to stage `in`: its member m writes stage1[in_idx_g[m][0]] times
+//   output 0: 1 (pivot 0) or beta (pivot 1),  output 1: beta s_m sgn (pivot 0) or s_m sgn (pivot 1),
+// with s_m the growth step's class sign and sgn the sign of its x = 1 term.  This reads those stage-1 values and
+// applies the coefficients, then accumulates A, B, C as group_trail_abc_pk does.
+template <int NTQ, int H>
+__device__ __forceinline__ void group_trail_fold_pk(const GroupArgs &ga, const GroupStepArgs &gg, const GroupStepArgs &gs,
+                                                    const uint64_t TB, const int L, const uint32_t in, const int gpiv,
+                                                    const float gbr, const float gbi, float (&acc)[4]) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - 1;
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1, gtpar = __popcll(TB & gg.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda, glam = (uint32_t)gg.lambda;
+    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    int j0 = 0, jstride = 1;
+    if (NG < blockDim.x) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(blockDim.x >> LG);
+    }
+    typedef FShape<NTQ, H, 0> S;
+    f32x2 SGT[NTQ];
+#pragma unroll
+    for (int t = 0; t < NTQ; t++) {
+        const float v = gs.par[t] ? -1.f : 1.f;
+        SGT[t] = f2_pack(v, v);
+    }
+    const float gsg = gg.par[0] ? -1.f : 1.f;
+    // growth-step coefficients: output 0 / output 1 (before the class sign of output 1)
+    const float c0r = gpiv == 0 ? 1.f : gbr, c0i = gpiv == 0 ? 0.f : gbi;
+    const float c1r = gpiv == 0 ? gbr * gsg : gsg, c1i = gpiv == 0 ? gbi * gsg : 0.f;
+    const float sig1 = (lam & 1u) ? -1.f : 1.f, gsig1 = (glam & 1u) ? -1.f : 1.f;
+    const f32x2 SGP = f2_pack(1.f, sig1), SGN = f2_pack(-1.f, -sig1);
+    const f32x2 GSP = f2_pack(1.f, gsig1), GSN = f2_pack(-1.f, -gsig1);
+    const f32x2 MONE = f2_pack(-1.f, -1.f);
+    f32x2 AA = 0ull, BB = 0ull, CR = 0ull, CI = 0ull;
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t ib[NTQ];
+        int gm[NTQ], tt[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            ib[t] = (uint32_t)ga.fsrc[j][t] * NC;
+            tt[t] = ga.ftau[j][t];
+            gm[t] = gtpar ^ gg.mpar[ga.fmem[j][t]];
+        }
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = 2u * g;
+            const int gpp = __popc(pc & glam);
+            f32x2 XR[2], XI[2], ZR[2], ZI[2];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib[t] + pc));
+                f32x2 VR = f2_pack(v.x, v.y), VI = f2_pack(v.z, v.w);
+                // the growth step's output value: coefficient (times its class sign for output 1)
+                float kr = tt[t] ? c1r : c0r, ki = tt[t] ? c1i : c0i;
+                f32x2 KR = f2_pack(kr, kr), KI = f2_pack(ki, ki);
+                if (tt[t]) {
+                    const f32x2 GS = ((gm[t] ^ gpp) & 1) ? GSN : GSP;
+                    KR = f2_mul(GS, KR);
+                    KI = f2_mul(GS, KI);
+                }
+                // the written step's operation order (group_cosets_pkf), so the values match its stores bit for bit
+                const f32x2 WR = f2_fma(f2_mul(KI, MONE), VI, f2_mul(KR, VR));
+                const f32x2 WI = f2_fma(KI, VR, f2_mul(KR, VI));
+                VR = WR;
+                VI = WI;
+                const int o0 = S::pout(t), o1 = S::qout(t);
+                const bool f0 = S::first_p(o0) == t, f1 = S::first_q(o1) == t;
+                if (f0) { XR[o0] = VR; XI[o0] = VI; }
+                else { XR[o0] = f2_add(XR[o0], VR); XI[o0] = f2_add(XI[o0], VI); }
+                if (f1) { ZR[o1] = f2_mul(SGT[t], VR); ZI[o1] = f2_mul(SGT[t], VI); }
+                else { ZR[o1] = f2_fma(SGT[t], VR, ZR[o1]); ZI[o1] = f2_fma(SGT[t], VI, ZI[o1]); }
+            }
+            const f32x2 SG = ((mp ^ __popc(pc & lam)) & 1) ? SGN : SGP;
+#pragma unroll
+            for (int tau = 0; tau < 2; tau++) {
+                const bool h0 = S::first_p(tau) >= 0, h1 = S::first_q(tau) >= 0;
+                if (h0) AA = f2_fma(XR[tau], XR[tau], f2_fma(XI[tau], XI[tau], AA));
+                if (h1) BB = f2_fma(ZR[tau], ZR[tau], f2_fma(ZI[tau], ZI[tau], BB));
+                if (h0 && h1) {
+                    const f32x2 SZR = f2_mul(SG, ZR[tau]), SZI = f2_mul(SG, ZI[tau]);
+                    CR = f2_fma(XR[tau], SZR, f2_fma(XI[tau], SZI, CR));
+                    CI = f2_fma(XI[tau], SZR, f2_fma(f2_mul(XR[tau], MONE), SZI, CI));
+                }
+            }
+        }
+    }
+    float a, b;
+    f2_unpack(AA, a, b); acc[0] += a + b;
+    f2_unpack(BB, a, b); acc[1] += a + b;
+    f2_unpack(CR, a, b); acc[2] += a + b;
+    f2_unpack(CI, a, b); acc[3] += a + b;
+}
+
+__device__ __forceinline__ void group_trail_fold(const GroupArgs &ga, const GroupStepArgs &gg, const GroupStepArgs &gs,
+                                                 const uint64_t TB, const int L, const uint32_t in, const int gpiv,
+                                                 const float gbr, const float gbi, float (&acc)[4]) {
+#define GSB_GT(NTQ_, H_) group_trail_fold_pk<NTQ_, H_>(ga, gg, gs, TB, L, in, gpiv, gbr, gbi, acc)
+    switch (gs.kind) {
+        case GK_1_0: GSB_GT(1, 0); break;
+        case GK_2_0: GSB_GT(2, 0); break;
+        case GK_2_1: GSB_GT(2, 1); break;
+        case GK_4_0: GSB_GT(4, 0); break;
+        case GK_4_1: GSB_GT(4, 1); break;
+        default: GSB_GT(4, 2); break;
+    }
+#undef GSB_GT
+}
+
 template <typename E, typename T, bool PK>
 __device__ __forceinline__ void group_trail64(const GroupArgs &ga, const GroupStepArgs &gs, const uint64_t TB,
                                               const int L, const uint32_t in, T (&acc)[4]) {
@@ -1229,7 +1349,7 @@ struct GroupSmem {
     uint32_t in0, in_bytes, mid[4], total;
 };
 template <typename E, typename T, int D, int TR>
-__host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L) {
+__host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L, bool fold = false) {
     typedef typename CplxOf<T>::type V;
     GroupSmem g{};
     const uint32_t NC = 1u << L;
@@ -1238,6 +1358,7 @@ __host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L) {
     uint32_t off = 16 + 2 * g.in_bytes;
     for (int s = 1; s <= D - 1 + TR; s++) {
         g.mid[s] = off;
+        if (fold && s == D) continue;   // the written stage is not kept (GroupArgs::fold)
         off += (uint32_t)ssz[s] * NC * (uint32_t)sizeof(V);
     }
     g.total = off;
@@ -1278,7 +1399,7 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
     }
     __syncthreads();
     if (!s_ok) return;
-    const GroupSmem sm = group_smem<E, T, D, TR>(ga.ssz, L);
+    const GroupSmem sm = group_smem<E, T, D, TR>(ga.ssz, L, ga.fold != 0);
     // Packed FP32 pairs pay where a trailing step evaluates both branch rows on the same coset sums (the sampling
     // passes, 3-7 % faster per pass).  A packed instruction holds the FMA pipe for two cycles, so passes without a
     // trailing step gain no throughput from it and lost up to 10 % to the extra register moves: they stay scalar.
@@ -1300,6 +1421,8 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
     // pass's scale, cp).  FP64 arithmetic (gsb_set_arith(64)) keeps the reference's complex64 arithmetic exactly:
     // full rotation, direct branch norms, the store the only rounding.
     constexpr bool FACT = sizeof(E) == 8 && std::is_same<T, float>::value;
+    // folded sampling passes (GroupArgs::fold) exist only in the two-CTA build: the three-CTA register cap spills them
+    constexpr bool FOLD = FACT && PK && D == 2 && TR == 1 && MINB == 2;
     int fpiv[D];
     T fsc[D], fbr[D], fbi[D];
     double fcp[D];
@@ -1409,7 +1532,12 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
         }
         if constexpr (FACT) {
             float2 *m64 = reinterpret_cast<float2 *>(mem);
-            if (D == 2) {
+            if (FOLD && ga.fold) {   // the written stage is not kept: the trailing step folds it
+                group_written64<T, false, false, true, false, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], 0u,
+                                                                 fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
+                                                                 fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
+                                                                 w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
+            } else if (D == 2) {
                 group_written64<T, false, false, true, TR == 1, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
                                                                    fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
                                                                    fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
@@ -1436,7 +1564,16 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
         if (TR) {
             if (D > 1) __syncthreads();
             const uint32_t(&tmid)[1] = D == 1 ? m1 : m2;
-            if (FACT && trail_abc)
+            bool done = false;
+            if constexpr (FOLD) {
+                if (ga.fold) {
+                    group_trail_fold(ga, ga.st[1], ga.st[2], TB, L, sm.mid[1], fpiv[D > 1 ? 1 : 0], fbr[D > 1 ? 1 : 0],
+                                     fbi[D > 1 ? 1 : 0], tabc);
+                    done = true;
+                }
+            }
+            if (done) {
+            } else if (FACT && trail_abc)
                 group_trail64<E, T, PK>(ga, ga.st[D], TB, L, tmid[0], tabc);
             else
                 group_cosets_any<E, T, false, false, false, 1, 2, PK>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
