@@ -110,6 +110,11 @@ static void *pick_group(int d, int tr) {
     if (tr) return d == 2 ? (void *)k_group<E, T, 2, 1> : (void *)k_group<E, T, 1, 1>;
     return d == 3 ? (void *)k_group<E, T, 3, 0> : (void *)k_group<E, T, 2, 0>;
 }
+// the warp-specialised instantiations (complex64, FP32 arithmetic, tiles of 2^9 classes or more)
+static void *pick_group_ws(int d, int tr) {
+    if (tr) return d == 2 ? (void *)k_group<float2, float, 2, 1, 2, true> : (void *)k_group<float2, float, 1, 1, 2, true>;
+    return d == 3 ? (void *)k_group<float2, float, 3, 0, 2, true> : (void *)k_group<float2, float, 2, 0, 2, true>;
+}
 // the three-CTAs-per-SM instantiations (complex64, FP32 arithmetic)
 static void *pick_group3(int d, int tr) {
     if (tr) return d == 2 ? (void *)k_group<float2, float, 2, 1, 3> : (void *)k_group<float2, float, 1, 1, 3>;
@@ -121,6 +126,8 @@ static void *pick_group3(int d, int tr) {
 struct Op {
     int k0 = 0, d = 1, tr = 0, lcap = 0;   // lcap: the tile-size cap the pass was built with (fused passes)
     int minb = 2;                          // CTAs per SM the fused kernel is built for (2, or 3: pick_group3)
+    int threads = GROUP_NCT;               // block size: GROUP_NCT, or GROUP_NCT + 32 (warp-specialised build)
+    int ws = 0;                            // the warp-specialised build (1) or not (0)
     bool group = false;
     bool norm_first = false;  // sampling: a norm pass of step k0 runs first (its bit has no other source)
     GroupArgs ga;
@@ -145,6 +152,7 @@ constexpr int GROUP_MIN_R = 12;                     // steps below 2^12 entries 
 // What a pass is, without its arguments: rebuilt with the current matrices whenever they change.
 struct OpShape {
     int k0 = 0, d = 1, tr = 0, lcap = 0, src = 0, minb = 2;
+    int ws = -1;   // warp-specialised build: 1 yes, 0 no, -1 the default rule (fill_group)
     bool group = false, norm_first = false;
 };
 constexpr uint32_t GROUP_SMEM_3 = 72 * 1024;        // shared memory of a fused-pass CTA when three share an SM
@@ -303,7 +311,7 @@ struct Engine {
         ga.withhold_loads = withhold_loads;
         void *memp = mem;
         void *kargs[] = {&ga, &memp, &c};
-        return cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3(256), kargs, op.smem, stream);
+        return cudaLaunchKernel(op.fn, dim3((unsigned)op.grid), dim3((unsigned)op.threads), kargs, op.smem, stream);
     }
 
     cudaError_t enqueue_item(int driver, bool use_forced, bool use_unif) {
@@ -515,7 +523,7 @@ static bool analytic_step(const HStep &hs) {
 
 // Group arguments of a fused pass from the host derivation and the steps' descriptors.  The pass writes stage gp.ws;
 // with gp.ws = gp.d - 1 the last step is the trailing norm step.
-static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_MAX_L, int minb = 2) {
+static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_MAX_L, int minb = 2, int ws_req = -1) {
     const HPlan &p = E.plan;
     const int D = gp.ws, TR = gp.d - gp.ws;
     if (gp.stage_size[0] > 32 || gp.stage_size[D] > 32) return false;
@@ -644,7 +652,11 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
         }
     }
     if (fold) {
-        ga.fold = 1;
+        // mode 2 when every trailing member reads one growth output in all its offsets
+        bool uni = true;
+        for (int j2 = 0; j2 < cs[2].nmem; j2++)
+            for (int t = 1; t < cs[2].ntq; t++) uni = uni && ftau[j2][t] == ftau[j2][0];
+        ga.fold = uni ? 2 : 1;
         memcpy(ga.fsrc, fsrc, sizeof fsrc);
         memcpy(ga.ftau, ftau, sizeof ftau);
         memcpy(ga.fmem, fmem, sizeof fmem);
@@ -657,13 +669,23 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
     op.minb = minb;
     op.smem = smem_at(L);
     op.ntiles = 1u << ga.nbhi;
+    // The warp-specialised build needs complex64 FP32 and tiles of 2^9 classes or more (a step thread's class pairs
+    // then are the same in every step).  By default the chain passes take it (complex64 chain 9.77 -> 9.29 ms per
+    // string of pass time on the headline plan); the sampling passes measured even with it (18.88 vs 18.89 ms, some
+    // passes faster, the folded ones 3 % slower), so there the autotuner times both.
+    const bool ws_ok = E.prec == 64 && E.arith == 32 && minb == 2 && L >= 9;
+    if (ws_req == 1 && !ws_ok) return false;
+    const bool ws = ws_ok && (ws_req < 0 ? TR == 0 : ws_req == 1);
+    op.ws = ws ? 1 : 0;
+    op.threads = ws ? GROUP_NCT + 32 : GROUP_NCT;
     if (E.prec == 128) op.fn = pick_group<double2, double>(op.d, op.tr);
     else if (E.arith == 64) op.fn = pick_group<float2, double>(op.d, op.tr);
-    else op.fn = minb == 3 ? pick_group3(op.d, op.tr) : pick_group<float2, float>(op.d, op.tr);
+    else if (minb == 3) op.fn = pick_group3(op.d, op.tr);
+    else op.fn = ws ? pick_group_ws(op.d, op.tr) : pick_group<float2, float>(op.d, op.tr);
     if (cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET) != cudaSuccess)
         return false;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, 256, op.smem) != cudaSuccess || nb < 1) nb = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, op.fn, op.threads, op.smem) != cudaSuccess || nb < 1) nb = 1;
     op.grid = (int)std::min<uint64_t>(op.ntiles, (uint64_t)nb * E.sms);
     op.entries = gp.entries_moved;
     return true;
@@ -685,7 +707,7 @@ static bool make_op(Engine &E, const OpShape &sh, Op &op) {
         return true;
     }
     GroupPlan gp;
-    if (!plan_group(E.plan, sh.k0, sh.d + sh.tr, 6, sh.lcap, gp, sh.d) || !fill_group(E, gp, op, sh.lcap, sh.minb))
+    if (!plan_group(E.plan, sh.k0, sh.d + sh.tr, 6, sh.lcap, gp, sh.d) || !fill_group(E, gp, op, sh.lcap, sh.minb, sh.ws))
         return false;
     op.norm_first = sh.norm_first;
     op.ga.src = sh.src;
@@ -1544,24 +1566,29 @@ static int autotune(Engine &E, int mode, int reps) {
     }
     // fused candidates starting at k, with their times (distinct tile sizes only)
     auto fused = [&](int k, int d, int tr, std::vector<std::pair<OpShape, double>> &out) -> int {
+        const bool c64f = E.prec == 64 && E.arith == 32;
         for (int minb : {2, 3}) {
-          if (minb == 3 && (E.prec != 64 || E.arith != 32)) continue;
-          int lastL = -1;
-          for (int lcap : {GROUP_MAX_L, GROUP_MAX_L - 1, GROUP_MAX_L - 2}) {
-            OpShape sh;
-            sh.group = true;
-            sh.k0 = k;
-            sh.d = d;
-            sh.tr = tr;
-            sh.lcap = lcap;
-            sh.minb = minb;
-            sh.src = GSRC_NORM;   // timing: the bit of step k as a norm pass would leave it
-            Op op;
-            if (!make_op(E, sh, op) || op.ga.L == lastL) continue;
-            lastL = op.ga.L;
-            const double t = timer([&] { return E.launch_op(op, drv, true, false); });
-            if (t < 0) return fail(GSB_E_CUDA, "autotuner: a timing launch failed");
-            out.push_back({sh, t});
+          if (minb == 3 && !c64f) continue;
+          for (int ws : {0, 1}) {   // the warp-specialised build: complex64 FP32, two CTAs per SM
+            if (ws && (minb != 2 || !c64f)) continue;
+            int lastL = -1;
+            for (int lcap : {GROUP_MAX_L, GROUP_MAX_L - 1, GROUP_MAX_L - 2}) {
+              OpShape sh;
+              sh.group = true;
+              sh.k0 = k;
+              sh.d = d;
+              sh.tr = tr;
+              sh.lcap = lcap;
+              sh.minb = minb;
+              sh.ws = ws;
+              sh.src = GSRC_NORM;   // timing: the bit of step k as a norm pass would leave it
+              Op op;
+              if (!make_op(E, sh, op) || op.ga.L == lastL) continue;
+              lastL = op.ga.L;
+              const double t = timer([&] { return E.launch_op(op, drv, true, false); });
+              if (t < 0) return fail(GSB_E_CUDA, "autotuner: a timing launch failed");
+              out.push_back({sh, t});
+            }
           }
         }
         return 0;

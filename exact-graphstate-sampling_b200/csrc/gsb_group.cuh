@@ -45,10 +45,11 @@ struct GroupArgs {
     uint64_t blk_out[32];  // written-stage offsets, bits >= L: output block i goes to the arena block at TB ^ blk_out[i]
     uint32_t z0lo[16][4];  // first step: member j, offset t -> bits < L of its stage-0 offset (position p ^ z0lo)
     uint32_t zdlo[16][2];  // last written step: member j, output tau -> bits < L of its offset
-    // fold = 1 (complex64 sampling passes of two written steps whose second is a one-offset growth step, GK_1_0): the
+    // fold = 1 or 2 (complex64 sampling passes of two written steps whose second is a one-offset growth step, GK_1_0): the
     // second step's outputs are not kept in shared memory; the trailing step reads the stage before it and applies
     // that step's map per term: its member j, offset t reads stage-1 value fsrc[j][t], output ftau[j][t] of the
-    // growth step's member fmem[j][t]
+    // growth step's member fmem[j][t].  fold = 2: every trailing member reads one output of the growth step in all
+    // its offsets (group_trail_fold2_pk)
     int fold;
     unsigned char fsrc[16][4], ftau[16][4], fmem[16][4];
     GroupStepArgs st[3];
@@ -67,15 +68,20 @@ template <> __device__ __forceinline__ float2 mkC<float2>(double r, double i) { 
 template <> __device__ __forceinline__ double2 mkC<double2>(double r, double i) { return make_double2(r, i); }
 __device__ __forceinline__ float2 mkCf(float r, float i) { return make_float2(r, i); }
 
+// Threads of a fused pass that run the steps: 256, the whole block, or (warp-specialised build) the first 256, with
+// one load-issuing warp after them.
+constexpr int GROUP_NCT = 256;
+
 // Grid-wide deterministic sums of ND values (same scheme as grid_reduce2); true in thread 0 of the last block.
+// Only the GROUP_NCT step threads contribute, so both builds sum in the same order.
 template <int ND>
 __device__ __forceinline__ bool grid_reduceN(double (&a)[ND], const Ctx &cx, double (&t)[ND]) {
     __shared__ double red[ND][32];
     __shared__ int last;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = GROUP_NCT / 32;
 #pragma unroll
     for (int i = 0; i < ND; i++) a[i] = warp_sum(a[i]);
-    if (lane == 0)
+    if (lane == 0 && warp < nw)
 #pragma unroll
         for (int i = 0; i < ND; i++) red[i][warp] = a[i];
     __syncthreads();
@@ -101,13 +107,13 @@ __device__ __forceinline__ bool grid_reduceN(double (&a)[ND], const Ctx &cx, dou
     double s[ND];
 #pragma unroll
     for (int i = 0; i < ND; i++) s[i] = 0;
-    for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+    for (unsigned int b = threadIdx.x; threadIdx.x < GROUP_NCT && b < gridDim.x; b += GROUP_NCT)
 #pragma unroll
         for (int i = 0; i < ND; i++) s[i] += __ldcg(cx.partials + ND * b + i);
 #pragma unroll
     for (int i = 0; i < ND; i++) s[i] = warp_sum(s[i]);
     __syncthreads();
-    if (lane == 0)
+    if (lane == 0 && warp < nw)
 #pragma unroll
         for (int i = 0; i < ND; i++) red[i][warp] = s[i];
     __syncthreads();
@@ -275,13 +281,13 @@ __device__ __forceinline__ void group_cosets(const GroupArgs &ga, const GroupSte
     const int m = ANY ? gs.m : 2;
     const int ntq = ANY ? gs.ntq : NTQ;
     const uint32_t lam = (uint32_t)gs.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     T sgn[NTQ];
     int ta0[NTQ], ta1[NTQ];
@@ -446,13 +452,13 @@ __device__ __forceinline__ void group_cosets_pk(const GroupArgs &ga, const Group
     const int m = ANY ? gs.m : 2;
     const int ntq = ANY ? gs.ntq : NTQ;
     const uint32_t lam = (uint32_t)gs.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     f32x2 sg[NTQ];
     int ta0[NTQ], ta1[NTQ];
@@ -621,13 +627,13 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
     const int tpar = __popcll(TB & gs.lambda) & 1;
     const int nm = gs.nmem;
     const uint32_t lam = (uint32_t)gs.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     T sg[NTQ];
 #pragma unroll
@@ -751,13 +757,13 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
     const int tpar = __popcll(TB & gs.lambda) & 1;
     const int nm = gs.nmem;
     const uint32_t lam = (uint32_t)gs.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     float sg[NTQ];
 #pragma unroll
@@ -924,13 +930,13 @@ __device__ __forceinline__ void group_trail_abc(const GroupArgs &ga, const Group
     const int tpar = __popcll(TB & gs.lambda) & 1;
     const int nm = gs.nmem;
     const uint32_t lam = (uint32_t)gs.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     T sg[NTQ];
 #pragma unroll
@@ -991,13 +997,13 @@ __device__ __forceinline__ void group_trail_abc_pk(const GroupArgs &ga, const Gr
     const int tpar = __popcll(TB & gs.lambda) & 1;
     const int nm = gs.nmem;
     const uint32_t lam = (uint32_t)gs.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     typedef FShape<NTQ, H, 0> S;
     f32x2 SGT[NTQ];
@@ -1065,13 +1071,13 @@ __device__ __forceinline__ void group_trail_fold_pk(const GroupArgs &ga, const G
     const int tpar = __popcll(TB & gs.lambda) & 1, gtpar = __popcll(TB & gg.lambda) & 1;
     const int nm = gs.nmem;
     const uint32_t lam = (uint32_t)gs.lambda, glam = (uint32_t)gg.lambda;
-    uint32_t g0 = threadIdx.x, gstride = blockDim.x;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
     int j0 = 0, jstride = 1;
-    if (NG < blockDim.x) {
+    if (NG < GROUP_NCT) {
         g0 = threadIdx.x & (NG - 1);
         gstride = NG;
         j0 = (int)(threadIdx.x >> LG);
-        jstride = (int)(blockDim.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
     }
     typedef FShape<NTQ, H, 0> S;
     f32x2 SGT[NTQ];
@@ -1148,14 +1154,199 @@ __device__ __forceinline__ void group_trail_fold_pk(const GroupArgs &ga, const G
     f2_unpack(CI, a, b); acc[3] += a + b;
 }
 
+// The folded trailing step when every trailing member reads one output tau of the growth step in all its offsets
+// (GroupArgs::fold = 2).  Those offsets then share the coefficient K (1 or beta, and the term sign), and their class
+// signs differ by the growth members' parities only (the class-dependent part is common), so
+//   A_j = |K|^2 A'_j, B_j = |K|^2 B'_j, C_j = |K|^2 C'_j,
+// with A', B', C' the sums over the stage-1 values times the relative signs r_t = s_t s_0: no complex products.
+template <int NTQ, int H>
+__device__ __forceinline__ void group_trail_fold2_pk(const GroupArgs &ga, const GroupStepArgs &gg, const GroupStepArgs &gs,
+                                                     const uint64_t TB, const int L, const uint32_t in, const int gpiv,
+                                                     const float gbr, const float gbi, float (&acc)[4]) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - 1;
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
+    int j0 = 0, jstride = 1;
+    if (NG < GROUP_NCT) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
+    }
+    typedef FShape<NTQ, H, 0> S;
+    // |K|^2 of the growth step's outputs: output 0 carries 1 (pivot 0) or beta (pivot 1), output 1 the other
+    const float bb = gbr * gbr + gbi * gbi;
+    const float kk0 = gpiv == 0 ? 1.f : bb, kk1 = gpiv == 0 ? bb : 1.f;
+    const float sig1 = (lam & 1u) ? -1.f : 1.f;
+    const f32x2 SGP = f2_pack(1.f, sig1), SGN = f2_pack(-1.f, -sig1);
+    const f32x2 MONE = f2_pack(-1.f, -1.f);
+    f32x2 AA = 0ull, BB = 0ull, CR = 0ull, CI = 0ull;
+    for (int j = j0; j < nm; j += jstride) {
+        const int mp = tpar ^ gs.mpar[j];
+        uint32_t ib[NTQ];
+        f32x2 RT[NTQ], ST[NTQ];
+        const int m0par = gg.mpar[ga.fmem[j][0]];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) {
+            ib[t] = (uint32_t)ga.fsrc[j][t] * NC;
+            // relative class sign of this offset's growth member (output 1 only: output 0 has no class sign)
+            const float r = (ga.ftau[j][0] && ((gg.mpar[ga.fmem[j][t]] ^ m0par) & 1)) ? -1.f : 1.f;
+            const float sq = gs.par[t] ? -r : r;
+            RT[t] = f2_pack(r, r);
+            ST[t] = f2_pack(sq, sq);
+        }
+        f32x2 aa = 0ull, bq = 0ull, cr = 0ull, ci = 0ull;
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = 2u * g;
+            f32x2 XR[2], XI[2], ZR[2], ZI[2];
+#pragma unroll
+            for (int t = 0; t < NTQ; t++) {
+                const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib[t] + pc));
+                const f32x2 VR = f2_pack(v.x, v.y), VI = f2_pack(v.z, v.w);
+                const int o0 = S::pout(t), o1 = S::qout(t);
+                const bool f0 = S::first_p(o0) == t, f1 = S::first_q(o1) == t;
+                if (f0) { XR[o0] = f2_mul(RT[t], VR); XI[o0] = f2_mul(RT[t], VI); }
+                else { XR[o0] = f2_fma(RT[t], VR, XR[o0]); XI[o0] = f2_fma(RT[t], VI, XI[o0]); }
+                if (f1) { ZR[o1] = f2_mul(ST[t], VR); ZI[o1] = f2_mul(ST[t], VI); }
+                else { ZR[o1] = f2_fma(ST[t], VR, ZR[o1]); ZI[o1] = f2_fma(ST[t], VI, ZI[o1]); }
+            }
+            const f32x2 SG = ((mp ^ __popc(pc & lam)) & 1) ? SGN : SGP;
+#pragma unroll
+            for (int tau = 0; tau < 2; tau++) {
+                const bool h0 = S::first_p(tau) >= 0, h1 = S::first_q(tau) >= 0;
+                if (h0) aa = f2_fma(XR[tau], XR[tau], f2_fma(XI[tau], XI[tau], aa));
+                if (h1) bq = f2_fma(ZR[tau], ZR[tau], f2_fma(ZI[tau], ZI[tau], bq));
+                if (h0 && h1) {
+                    const f32x2 SZR = f2_mul(SG, ZR[tau]), SZI = f2_mul(SG, ZI[tau]);
+                    cr = f2_fma(XR[tau], SZR, f2_fma(XI[tau], SZI, cr));
+                    ci = f2_fma(XI[tau], SZR, f2_fma(f2_mul(XR[tau], MONE), SZI, ci));
+                }
+            }
+        }
+        const float k = ga.ftau[j][0] ? kk1 : kk0;
+        const f32x2 KK = f2_pack(k, k);
+        AA = f2_fma(KK, aa, AA);
+        BB = f2_fma(KK, bq, BB);
+        CR = f2_fma(KK, cr, CR);
+        CI = f2_fma(KK, ci, CI);
+    }
+    float a, b;
+    f2_unpack(AA, a, b); acc[0] += a + b;
+    f2_unpack(BB, a, b); acc[1] += a + b;
+    f2_unpack(CR, a, b); acc[2] += a + b;
+    f2_unpack(CI, a, b); acc[3] += a + b;
+}
+
+// The shared sums of a trailing step of shape GK_2_1 (offset 0's x = 0 term to output 0, offset 1's to output 1, the
+// x = 1 terms to the other output), packed FP32.  With W_t the value offset t reads:
+//   X_0 = W_0, X_1 = W_1, Z_0 = sg_1 W_1, Z_1 = sg_0 W_0, so A = B = sum |W_0|^2 + |W_1|^2 and
+//   C = sum SG (sg_1 P + sg_0 conj(P)), P = W_0 conj(W_1), SG the class sign:
+// two squared norms and one complex product per class pair instead of the output sums.  FOLD (GroupArgs::fold): W_t
+// is K_t s_t V_t, a growth output (K_t its coefficient, s_t its class sign for output 1) of the stage-1 value V_t;
+// then A = sum |K_0|^2 |V_0|^2 + |K_1|^2 |V_1|^2 and P = K_0 conj(K_1) s_0 s_1 V_0 conj(V_1), and the class signs
+// SG s_0 s_1 of a pair reduce to the parity of (a member constant) ^ popc(pc & msk).
+template <bool FOLD>
+__device__ __forceinline__ void group_trail21_pk(const GroupArgs &ga, const GroupStepArgs &gg, const GroupStepArgs &gs,
+                                                 const uint64_t TB, const int L, const uint32_t in, const int gpiv,
+                                                 const float gbr, const float gbi, float (&acc)[4]) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t NC = 1u << L;
+    const int LG = L - 1;
+    const uint32_t NG = 1u << LG;
+    const int tpar = __popcll(TB & gs.lambda) & 1;
+    const int nm = gs.nmem;
+    const uint32_t lam = (uint32_t)gs.lambda;
+    uint32_t g0 = threadIdx.x, gstride = GROUP_NCT;
+    int j0 = 0, jstride = 1;
+    if (NG < GROUP_NCT) {
+        g0 = threadIdx.x & (NG - 1);
+        gstride = NG;
+        j0 = (int)(threadIdx.x >> LG);
+        jstride = (int)(GROUP_NCT >> LG);
+    }
+    const float sg0 = gs.par[0] ? -1.f : 1.f, sg1 = gs.par[1] ? -1.f : 1.f;
+    const float csum = sg0 + sg1, cdif = sg1 - sg0;
+    // growth-step coefficients (FOLD): output 0 / output 1 before its class sign
+    float c0r = 1.f, c0i = 0.f, c1r = 1.f, c1i = 0.f;
+    uint32_t glam = 0;
+    int gtpar = 0;
+    if (FOLD) {
+        const float gsg = gg.par[0] ? -1.f : 1.f;
+        c0r = gpiv == 0 ? 1.f : gbr;
+        c0i = gpiv == 0 ? 0.f : gbi;
+        c1r = gpiv == 0 ? gbr * gsg : gsg;
+        c1i = gpiv == 0 ? gbi * gsg : 0.f;
+        glam = (uint32_t)gg.lambda;
+        gtpar = __popcll(TB & gg.lambda) & 1;
+    }
+    const f32x2 MONE = f2_pack(-1.f, -1.f);
+    f32x2 AA = 0ull, CR = 0ull, CI = 0ull;
+    for (int j = j0; j < nm; j += jstride) {
+        uint32_t ib0, ib1, msk = lam;
+        int cst = tpar ^ gs.mpar[j];
+        float k0 = 1.f, k1 = 1.f, kr = 1.f, ki = 0.f;
+        if (FOLD) {
+            ib0 = (uint32_t)ga.fsrc[j][0] * NC;
+            ib1 = (uint32_t)ga.fsrc[j][1] * NC;
+            const int t0 = ga.ftau[j][0], t1 = ga.ftau[j][1];
+            if (t0) cst ^= gtpar ^ gg.mpar[ga.fmem[j][0]];
+            if (t1) cst ^= gtpar ^ gg.mpar[ga.fmem[j][1]];
+            if (t0 != t1) msk ^= glam;
+            const float ar = t0 ? c1r : c0r, ai = t0 ? c1i : c0i, br = t1 ? c1r : c0r, bi = t1 ? c1i : c0i;
+            k0 = ar * ar + ai * ai;
+            k1 = br * br + bi * bi;
+            kr = ar * br + ai * bi;   // K_0 conj(K_1)
+            ki = ai * br - ar * bi;
+        } else {
+            ib0 = (uint32_t)gs.in_idx[j][0] * NC;
+            ib1 = (uint32_t)gs.in_idx[j][1] * NC;
+        }
+        const float s1 = (msk & 1u) ? -1.f : 1.f;
+        const f32x2 SGP = f2_pack(1.f, s1), SGN = f2_pack(-1.f, -s1);
+        f32x2 a0 = 0ull, a1 = 0ull, qr = 0ull, qi = 0ull;
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = 2u * g;
+            const float4 u = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib0 + pc));
+            const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib1 + pc));
+            const f32x2 UR = f2_pack(u.x, u.y), UI = f2_pack(u.z, u.w), VR = f2_pack(v.x, v.y), VI = f2_pack(v.z, v.w);
+            a0 = f2_fma(UR, UR, f2_fma(UI, UI, a0));
+            a1 = f2_fma(VR, VR, f2_fma(VI, VI, a1));
+            const f32x2 SG = ((cst ^ __popc(pc & msk)) & 1) ? SGN : SGP;
+            const f32x2 PR = f2_fma(UR, VR, f2_mul(UI, VI));             // Re U conj(V)
+            const f32x2 PI = f2_fma(UI, VR, f2_mul(f2_mul(UR, MONE), VI));  // Im U conj(V)
+            qr = f2_fma(SG, PR, qr);
+            qi = f2_fma(SG, PI, qi);
+        }
+        AA = f2_fma(f2_pack(k0, k0), a0, f2_fma(f2_pack(k1, k1), a1, AA));
+        // C += sg_1 K Q + sg_0 conj(K Q), K = K_0 conj(K_1), Q = (qr, qi)
+        const f32x2 KR = f2_pack(kr, kr), KI = f2_pack(ki, ki);
+        const f32x2 QR = f2_fma(KR, qr, f2_mul(f2_mul(KI, MONE), qi)), QI = f2_fma(KR, qi, f2_mul(KI, qr));
+        CR = f2_fma(f2_pack(csum, csum), QR, CR);
+        CI = f2_fma(f2_pack(cdif, cdif), QI, CI);
+    }
+    float a, b;
+    f2_unpack(AA, a, b);
+    acc[0] += a + b;
+    acc[1] += a + b;
+    f2_unpack(CR, a, b); acc[2] += a + b;
+    f2_unpack(CI, a, b); acc[3] += a + b;
+}
+
 __device__ __forceinline__ void group_trail_fold(const GroupArgs &ga, const GroupStepArgs &gg, const GroupStepArgs &gs,
                                                  const uint64_t TB, const int L, const uint32_t in, const int gpiv,
                                                  const float gbr, const float gbi, float (&acc)[4]) {
-#define GSB_GT(NTQ_, H_) group_trail_fold_pk<NTQ_, H_>(ga, gg, gs, TB, L, in, gpiv, gbr, gbi, acc)
+#define GSB_GT(NTQ_, H_)                                                                  \
+    (ga.fold == 2 ? group_trail_fold2_pk<NTQ_, H_>(ga, gg, gs, TB, L, in, gpiv, gbr, gbi, acc) \
+                  : group_trail_fold_pk<NTQ_, H_>(ga, gg, gs, TB, L, in, gpiv, gbr, gbi, acc))
     switch (gs.kind) {
         case GK_1_0: GSB_GT(1, 0); break;
         case GK_2_0: GSB_GT(2, 0); break;
-        case GK_2_1: GSB_GT(2, 1); break;
+        case GK_2_1: group_trail21_pk<true>(ga, gg, gs, TB, L, in, gpiv, gbr, gbi, acc); break;
         case GK_4_0: GSB_GT(4, 0); break;
         case GK_4_1: GSB_GT(4, 1); break;
         default: GSB_GT(4, 2); break;
@@ -1171,7 +1362,7 @@ __device__ __forceinline__ void group_trail64(const GroupArgs &ga, const GroupSt
         switch (gs.kind) {
             case GK_1_0: GSB_GT(1, 0); break;
             case GK_2_0: GSB_GT(2, 0); break;
-            case GK_2_1: GSB_GT(2, 1); break;
+            case GK_2_1: group_trail21_pk<false>(ga, gs, gs, TB, L, in, 0, 0.f, 0.f, acc); break;
             case GK_4_0: GSB_GT(4, 0); break;
             case GK_4_1: GSB_GT(4, 1); break;
             default: GSB_GT(4, 2); break;
@@ -1320,6 +1511,9 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
         : "memory");
     return done != 0;
 }
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
 // global -> shared, completion counted on the mbarrier (bytes: multiple of 16, both addresses 16-byte aligned)
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
@@ -1342,7 +1536,8 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity,
 }
 
 // Shared-memory layout of a fused pass (bytes; every buffer 16-byte aligned):
-//   [0, 16)  two mbarriers (one per input buffer)
+//   [0, 32)  four mbarriers: per input buffer, its loads landed; and (warp-specialised build) every step warp is done
+//            reading it
 //   two input tiles   ssz[0] blocks of 2^L arena entries (E), block i = arena block at TB ^ blk_in[i]
 //   stages 1 .. D-1 (and D when a step trails it): [value index][class] (CplxOf<T>)
 struct GroupSmem {
@@ -1353,9 +1548,9 @@ __host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L, bool
     typedef typename CplxOf<T>::type V;
     GroupSmem g{};
     const uint32_t NC = 1u << L;
-    g.in0 = 16;
+    g.in0 = 32;
     g.in_bytes = (uint32_t)ssz[0] * NC * (uint32_t)sizeof(E);
-    uint32_t off = 16 + 2 * g.in_bytes;
+    uint32_t off = 32 + 2 * g.in_bytes;
     for (int s = 1; s <= D - 1 + TR; s++) {
         g.mid[s] = off;
         if (fold && s == D) continue;   // the written stage is not kept (GroupArgs::fold)
@@ -1375,8 +1570,13 @@ __host__ __device__ inline GroupSmem group_smem(const int (&ssz)[4], int L, bool
 // MINB CTAs per SM: 2 by default (up to 128 registers a thread: without this bound the compiler kept some
 // instantiations at 64-80 registers and spilled); 3 for complex64 FP32 passes with tiles small enough for three
 // CTAs' shared memory (85 registers: more resident warps to hide the dependent arithmetic), an autotuner candidate.
-template <typename E, typename T, int D, int TR, int MINB = 2>
-__global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
+// WS (warp-specialised build, complex64 FP32 passes with tiles of 2^9 classes or more): 256 step threads and one
+// load-issuing warp.  From 2^9 classes a step thread handles the same class pairs in every step of the pass, so the
+// stages between steps are private to it and need no barrier; the input buffers are handed over by mbarriers (loads
+// landed / every step warp done reading), so the step warps do not wait for one another within or between tiles.
+template <typename E, typename T, int D, int TR, int MINB = 2, bool WS = false>
+__global__ void __launch_bounds__(WS ? GROUP_NCT + 32 : GROUP_NCT, MINB)
+    k_group(const GroupArgs ga, E *__restrict__ mem, const Ctx cx) {
     DevState *st = cx.st;
     if (*(volatile int *)&st->dead) return;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -1423,6 +1623,7 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
     constexpr bool FACT = sizeof(E) == 8 && std::is_same<T, float>::value;
     // folded sampling passes (GroupArgs::fold) exist only in the two-CTA build: the three-CTA register cap spills them
     constexpr bool FOLD = FACT && PK && D == 2 && TR == 1 && MINB == 2;
+    static_assert(!WS || (FACT && MINB == 2), "warp-specialised build: complex64 FP32, two CTAs per SM");
     int fpiv[D];
     T fsc[D], fbr[D], fbi[D];
     double fcp[D];
@@ -1469,6 +1670,10 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
     if (threadIdx.x == 0) {
         mbar_init(bar0, 1);
         mbar_init(bar0 + 8, 1);
+        if (WS) {
+            mbar_init(bar0 + 16, GROUP_NCT / 32);
+            mbar_init(bar0 + 24, GROUP_NCT / 32);
+        }
         mbar_init_fence();
     }
     __syncthreads();
@@ -1482,7 +1687,7 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
     int issued = 0;   // tiles whose loads thread 0 issued
     // test hook: 1 withholds every CTA's tile loads, 2 only those of the odd CTAs (a partial failure)
     const bool withhold = ga.withhold_loads == 1 || (ga.withhold_loads == 2 && (blockIdx.x & 1u));
-    if (threadIdx.x == 0 && !withhold)
+    if (!WS && threadIdx.x == 0 && !withhold)
         for (unsigned int n = i0; n < i1 && n < i0 + 2; n++) {
             issue_loads(n, tile_tb(n));
             issued++;
@@ -1490,14 +1695,44 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
     int waited = 0;   // tiles whose loads completed
     bool failed = false;
     uint64_t tb = i0 < i1 ? tile_tb(i0) : 0;
+    if (WS && threadIdx.x >= GROUP_NCT) {
+        // the load-issuing warp: tile n goes into buffer (n - i0) & 1 once every step warp is done with tile n - 2
+        if (threadIdx.x == GROUP_NCT && !withhold) {
+            uint64_t tp = tb;
+            unsigned int n = i0;
+            for (; n < i1; n++) {
+                const uint32_t b = (n - i0) & 1;
+                if (n >= i0 + 2 && !mbar_wait_bounded(bar0 + 16 + 8 * b, ((n - i0 - 2) >> 1) & 1, &s_abort)) {
+                    s_abort = 1;
+                    break;
+                }
+                issue_loads(n, tp);
+                if (n + 1 < i1) tp ^= ga.bhi[__ffs((int)(n + 1)) - 1] & ~mask;
+            }
+            // the last tile issued into each buffer has landed before the block goes on (bounded): nothing is in
+            // flight into this block's shared memory when it leaves
+            volatile int never = 0;
+            for (unsigned int m = n >= i0 + 2 ? n - 2 : i0; m < n; m++)
+                mbar_wait_bounded(bar0 + 8 * ((m - i0) & 1), ((m - i0) >> 1) & 1, &never);
+        }
+    } else
     for (unsigned int it = i0; it < i1; it++) {
         const int buf = (int)((it - i0) & 1);
         const uint64_t TB = tb;
-        if (!mbar_wait_bounded(bar0 + 8 * (uint32_t)buf, ((it - i0) >> 1) & 1, &s_abort)) s_abort = 1;
-        __syncthreads();
-        if (s_abort) {
-            failed = true;
-            break;
+        if constexpr (WS) {
+            // one decision per warp: a warp whose wait ran out stops, and the others' waits see s_abort
+            if (!__all_sync(0xffffffffu, mbar_wait_bounded(bar0 + 8 * (uint32_t)buf, ((it - i0) >> 1) & 1, &s_abort))) {
+                s_abort = 1;
+                failed = true;
+                break;
+            }
+        } else {
+            if (!mbar_wait_bounded(bar0 + 8 * (uint32_t)buf, ((it - i0) >> 1) & 1, &s_abort)) s_abort = 1;
+            __syncthreads();
+            if (s_abort) {
+                failed = true;
+                break;
+            }
         }
         waited++;
         T ns[D][1][1];
@@ -1515,15 +1750,18 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
             else
                 group_written64<T, true, true, false, true, PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
                                                                fsc[0], fbr[0], fbi[0], w[0], wj[0], ns[0][0][0]);
-            __syncthreads();
         } else if (D == 1) {
             group_cosets_any<E, T, true, true, TR == 1, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
-            __syncthreads();
         } else {
             group_cosets_any<E, T, true, false, true, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
+        }
+        if constexpr (WS) {
+            __syncwarp();
+            if ((threadIdx.x & 31) == 0) mbar_arrive(bar0 + 16 + 8 * (uint32_t)buf);   // this warp is done with the tile
+        } else {
             __syncthreads();
         }
-        if (threadIdx.x == 0 && it + 2 < i1 && !withhold) {
+        if (!WS && threadIdx.x == 0 && it + 2 < i1 && !withhold) {
             // tile it + 2 is two Gray-code steps from this tile (gray(n + 1) = gray(n) ^ 2^ctz(n + 1)); rebuilding its
             // base from the index, a loop over the class-base vectors, held up warp 0 and so every warp at the next
             // barrier (4-7 % of the pass)
@@ -1547,7 +1785,7 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
                                                                  fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
                                                                  fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
                                                                  w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
-                __syncthreads();
+                if constexpr (!WS) __syncthreads();
                 group_written64<T, false, false, true, false, PK>(ga, ga.st[2], m64, TB, L, sm.mid[2], 0u,
                                                                  fpiv[D > 2 ? 2 : 0], fsc[D > 2 ? 2 : 0],
                                                                  fbr[D > 2 ? 2 : 0], fbi[D > 2 ? 2 : 0],
@@ -1562,7 +1800,7 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
         }
         T tabc[4] = {0, 0, 0, 0};
         if (TR) {
-            if (D > 1) __syncthreads();
+            if (D > 1 && !WS) __syncthreads();
             const uint32_t(&tmid)[1] = D == 1 ? m1 : m2;
             bool done = false;
             if constexpr (FOLD) {
@@ -1578,7 +1816,7 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
             else
                 group_cosets_any<E, T, false, false, false, 1, 2, PK>(ga, ga.st[D], mem, TB, L, tmid, none2, tr_r, tr_i, nt);
         }
-        __syncthreads();
+        if constexpr (!WS) __syncthreads();
 #pragma unroll
         for (int s = 0; s < D; s++) acc[s] += (double)ns[s][0][0];
         if (TR) {
@@ -1592,13 +1830,19 @@ __global__ void __launch_bounds__(256, MINB) k_group(const GroupArgs ga, E *__re
         }
         if (it + 1 < i1) tb ^= ga.bhi[__ffs((int)(it + 1)) - 1] & ~mask;
     }
+    if constexpr (WS) {
+        __syncthreads();   // every warp has left its loop (each wait is bounded); the load warp has drained its loads
+        failed = s_abort != 0;
+    }
     if (failed) {
         // a load never completed: record it, let the loads still in flight land (bounded) and leave the item
         if (threadIdx.x == 0) {
             atomicExch(&st->err, 1);
             st->dead = 1;
             volatile int never = 0;
-            for (int n = waited; n < issued; n++) mbar_wait_bounded(bar0 + 8 * (uint32_t)(n & 1), (uint32_t)(n >> 1) & 1, &never);
+            if (!WS)
+                for (int n = waited; n < issued; n++)
+                    mbar_wait_bounded(bar0 + 8 * (uint32_t)(n & 1), (uint32_t)(n >> 1) & 1, &never);
             // count this block as finished, so the block that finishes last (a failed one or one in grid_reduceN)
             // sees every block and returns the counter to zero
             __threadfence();
