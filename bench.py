@@ -30,6 +30,7 @@ own strings on its own GPU; value = all ranks' amplitudes / the slowest rank's t
   wide34: n = 80, width 34 (2^34-entry complex64 arena, 137 GB): 256 amplitudes and 16 exact samples.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -88,6 +89,10 @@ def parse():
     ap.add_argument("--form", default="headline", choices=["headline", "batch", "grad", "wide34", "hybrid"],
                     help="workload to measure (the default line is the headline n = 70, width-30 workload)")
     ap.add_argument("--batch-instances", type=int, default=512)
+    ap.add_argument("--wide34-amps", type=int, default=256, help="--form wide34: amplitudes timed")
+    ap.add_argument("--wide34-samples", type=int, default=16, help="--form wide34: exact samples timed")
+    ap.add_argument("--no-wide34-check", dest="wide34_check", action="store_false",
+                    help="--form wide34: skip the complex128 cross-check through the width-30 sliced order")
     ap.add_argument("--batch-order", default="qubit", choices=["qubit", "search"],
                     help="--form batch: qubit index order (widths 7-20, the configuration's) or the native search")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
@@ -533,15 +538,22 @@ def run_gsb(args):
                                              + (f", -march=x86-64-{ref_isa(64)}" if kind == "reference" else "") + ")",
                                    "abs_dlog2p_vs_gpu_c128": abs(ref_lp - float(lp128[W * A])) if c128 else None}
     if rank == 0 and world == 1 and args.forms:
-        # the hybrid driver and the batched launch on the same GPU, reported inside this line
+        # the hybrid driver, the batched launch, the adjoint sweep and the width-34 arena on the same GPU, reported
+        # inside this line (the width-34 form with 16 amplitudes and 4 samples, without its sliced complex128
+        # cross-check, which `--form wide34` runs); the width-30 engines are closed, so the 137 GB arena fits
+        torch.cuda.empty_cache()
         out["forms"] = {}
-        for name, fn in (("hybrid", run_form_hybrid), ("batch", run_form_batch)):
+        for name, fn in (("hybrid", run_form_hybrid), ("batch", run_form_batch), ("grad", run_form_grad),
+                         ("wide34", run_form_wide34)):
             try:
                 sub = argparse.Namespace(**vars(args))
                 sub.steps, sub.warmup = 5, 3
+                sub.wide34_amps, sub.wide34_samples, sub.wide34_check = 16, 4, False
                 out["forms"][name] = fn(sub, emit=False)
             except Exception as ex:   # a reported extra only
                 out["forms"][name] = {"unavailable": str(ex)[:200]}
+            gc.collect()
+            torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps(out), flush=True)
     replicas.finish(world)
@@ -625,7 +637,7 @@ def run_form_batch(args, emit=True):
                }, emit=emit)
 
 
-def run_form_grad(args):
+def run_form_grad(args, emit=True):
     """Gradient of -mean log2 Pr over 2048 exact targets w.r.t. the 48 x 3 rotation angles (adjoint sweep)."""
     import math
     import numpy as np
@@ -659,18 +671,20 @@ def run_form_grad(args):
     bwd = sum(2 * (1 << s["r"]) + (1 << s["rn"]) for s in w["steps"])
     byt = 16.0 * len(bits) * (2 * fwd + bwd)
     peak, kind = peaks()
-    _form_line("grad", "s per loss+gradient, n=48 rotation layer, 2048 exact targets", t, "s", False, {
+    sweep.close()
+    return _form_line("grad", "s per loss+gradient, n=48 rotation layer, 2048 exact targets", t, "s", False, {
         "roofline": {"bound": "hbm", "achieved": byt / t / 1e9, "peak": peak, "unit": "GB/s", "frac": byt / t / 1e9 / peak,
                      "peak_kind": kind, "bytes_per_string": byt / len(bits)},
         "strings_per_s": len(bits) / t, "loss": loss.item(), "grad_norm": float(theta.grad.norm()),
         "step_times_s": [round(x, 4) for x in times],
         "width": w["width"], "checkpoint_every": 4, "dtype": "c128 arena, f64",
         "targets": "2048 exact samples of a second seeded n=48 instance (complex128 executor)",
-        "steps": args.steps, "warmup": max(3, args.warmup)})
+        "steps": args.steps, "warmup": max(3, args.warmup)}, emit=emit)
 
 
-def run_form_wide34(args):
-    """n = 80, width 34 in complex64: 256 amplitudes and 16 exact samples on one GPU."""
+def run_form_wide34(args, emit=True):
+    """n = 80, width 34 in complex64: 256 amplitudes and 16 exact samples on one GPU (fewer with --wide34-amps /
+    --wide34-samples), and 4 amplitudes against complex128 through a width-30 sliced order (--no-wide34-check: none)."""
     import numpy as np
     import torch
     import gsb
@@ -679,7 +693,8 @@ def run_form_wide34(args):
     w = workloads.wide34_instance()
     t_plan = time.perf_counter() - t0
     ns = len(w["steps"])
-    strings = workloads.random_strings(ns, 256, seed=2024)
+    NA, NS = args.wide34_amps, args.wide34_samples
+    strings = workloads.random_strings(ns, 256, seed=2024)[:NA]
     with gsb.Engine.from_text(w["plan"], precision=gsb.GSB_C64) as eng:
         stream = torch.cuda.Stream()
         eng.set_stream(stream.cuda_stream)
@@ -688,13 +703,35 @@ def run_form_wide34(args):
         lp, _ = eng.chain(strings)
         t_amp = time.perf_counter() - t1
         t2 = time.perf_counter()
-        sbits, slp = eng.sample(16, seed=7)
+        sbits, slp = eng.sample(NS, seed=7)
         t_smp = time.perf_counter() - t2
         chain_bytes = 8.0 * float(eng.fusion_groups()[1].sum())     # bytes the executed passes move per string
         sample_bytes = 8.0 * float(eng.sample_groups()[1].sum())
-    # complex128 cross-check of 4 amplitudes: a second order with 10 slice vertices cut out (width 30), every
-    # slice's final table from 'prefix' through the last step, summed by 'resume' (the reference's slicing identity,
-    # gsamp2.cpp:176-208); one complex128 arena serves all 1,024 slice plans (they differ only in M)
+    check_line = {"skipped": "--no-wide34-check"}
+    if args.wide34_check:
+        check_line = wide34_sliced_check(w, strings[:4], lp[:4])
+    return _form_line("wide34", "amps/s and s/sample at n=80, width 34, complex64 (137 GB arena)", NA / t_amp, "amps/s",
+                      True, {
+        "s_per_sample": t_smp / NS, "amplitudes": NA, "samples": NS, "width": w["width"],
+        "arena_gb": (1 << w["width"]) * 8 / 1e9,
+        "log2p_first": [float(x) for x in lp[:4]], "sample_log2p": [float(x) for x in slp[:4]],
+        "dtype": "c64 arena, f32 sums, f64 norms/scales", "host_planning_s": t_plan,
+        "timing": "wall clock around the host-buffer C-ABI calls (whole batches, one synchronisation each)",
+        "roofline": {"bound": "hbm", "achieved": NA * chain_bytes / t_amp / 1e9, "peak": peaks()[0], "unit": "GB/s",
+                     "frac": NA * chain_bytes / t_amp / 1e9 / peaks()[0], "peak_kind": peaks()[1],
+                     "pass_bytes_per_string": chain_bytes, "sample_pass_bytes": sample_bytes,
+                     "sample_achieved": NS * sample_bytes / t_smp / 1e9,
+                     "note": "wall clock (host calls included), so a lower bound on the kernels' rate"},
+        "c128_sliced_check": check_line}, emit=emit)
+
+
+def wide34_sliced_check(w, strings, lp):
+    """complex128 cross-check of 4 amplitudes of the width-34 instance: a second order with 10 slice vertices cut out
+    (width 30), every slice's final table from 'prefix' through the last step, summed by 'resume' (the reference's
+    slicing identity, gsamp2.cpp:176-208); one complex128 arena serves all 1,024 slice plans (they differ only in M)"""
+    import numpy as np
+    import gsb
+    import workloads
     t3 = time.perf_counter()
     sl = workloads.wide34_slices(w)
     v1 = [s["v"] for s in w["steps"]]
@@ -719,20 +756,9 @@ def run_form_wide34(args):
             _, lpf, _, _ = e128.resume(line, ns2, 0, 0, dumps[i], lss[i])
             check.append((float(lp[i]), float(lpf)))
     t_check = time.perf_counter() - t3
-    _form_line("wide34", "amps/s and s/sample at n=80, width 34, complex64 (137 GB arena)", 256 / t_amp, "amps/s", True, {
-        "s_per_sample": t_smp / 16, "width": w["width"], "arena_gb": (1 << w["width"]) * 8 / 1e9,
-        "log2p_first": [float(x) for x in lp[:4]], "sample_log2p": [float(x) for x in slp[:4]],
-        "dtype": "c64 arena, f32 sums, f64 norms/scales", "host_planning_s": t_plan,
-        "timing": "wall clock around the host-buffer C-ABI calls (whole batches, one synchronisation each)",
-        "roofline": {"bound": "hbm", "achieved": 256 * chain_bytes / t_amp / 1e9, "peak": peaks()[0], "unit": "GB/s",
-                     "frac": 256 * chain_bytes / t_amp / 1e9 / peaks()[0], "peak_kind": peaks()[1],
-                     "pass_bytes_per_string": chain_bytes, "sample_pass_bytes": sample_bytes,
-                     "sample_achieved": 16 * sample_bytes / t_smp / 1e9,
-                     "note": "wall clock (host calls included), so a lower bound on the kernels' rate"},
-        "c128_sliced_check": {"slices": len(sl["plans"]), "slice_vertices": sl["S"], "width": sl["width"],
-                              "arena_gb": (1 << sl["width"]) * 16 / 1e9,
-                              "log2p_c64_vs_c128": check,
-                              "max_abs_dlog2p": max(abs(a - b) for a, b in check), "seconds": t_check}})
+    return {"slices": len(sl["plans"]), "slice_vertices": sl["S"], "width": sl["width"],
+            "arena_gb": (1 << sl["width"]) * 16 / 1e9, "log2p_c64_vs_c128": check,
+            "max_abs_dlog2p": max(abs(a - b) for a, b in check), "seconds": t_check}
 
 
 def run_form_hybrid(args, emit=True):

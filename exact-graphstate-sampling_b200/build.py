@@ -5,6 +5,7 @@
 nvcc cross-compiles for sm_100a without a GPU, so this runs on any machine with the CUDA toolkit.  Outputs sit next
 to this file, where gsb.py loads them.
 """
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -45,9 +46,18 @@ def _run(cmd):
 def build(force=False, verbose_ptxas=False):
     deps = [os.path.join(CSRC, f) for f in LIB_DEPS] + [os.path.join(INCLUDE, "gsb.h")]
     if force or _stale(LIB, deps):
-        cmd = [_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else []) + \
-              ["-shared", "-I" + INCLUDE, "-I" + CSRC, "-o", LIB] + [os.path.join(CSRC, f) for f in LIB_SOURCES]
-        _run(cmd)
+        # one object per source, compiled in parallel (the sources share no device code), then one link
+        objdir = os.path.join(ROOT, "_build", "gsb")
+        os.makedirs(objdir, exist_ok=True)
+        cmds, objs = [], []
+        for f in LIB_SOURCES:
+            obj = os.path.join(objdir, f + ".o")
+            objs.append(obj)
+            cmds.append([_nvcc()] + NVCC_FLAGS + (["-Xptxas", "-v"] if verbose_ptxas else []) +
+                        ["-c", "-I" + INCLUDE, "-I" + CSRC, "-o", obj, os.path.join(CSRC, f)])
+        with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+            list(ex.map(_run, cmds))
+        _run([_nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB] + objs)
     cli_src = os.path.join(CSRC, "gsb_cli.cpp")
     if force or _stale(CLI, [cli_src, LIB, os.path.join(INCLUDE, "gsb.h")]):
         _run(["g++", "-O2", "-std=c++17", "-Wall", "-I" + INCLUDE, cli_src, "-L" + HERE, "-lgsb",

@@ -187,6 +187,8 @@ struct Engine {
     void *d_dump = nullptr;
     size_t dump_bytes = 0;
     std::vector<StepArgs> args;
+    StepArgs *d_args = nullptr;          // device copy of args (read by the small-step runs, k_small_run)
+    bool args_dirty = true;              // args changed since d_args was last written
     std::vector<Launch> lw, ln;
     std::map<int, cudaGraphExec_t> graphs;   // key: graph kind
     std::map<void *, int> occ;
@@ -210,6 +212,7 @@ struct Engine {
         DevGuard g(dev);
         for (auto &kv : graphs) cudaGraphExecDestroy(kv.second);
         cudaFree(mem);
+        cudaFree(d_args);
         cudaFree(st);
         cudaFree(partials);
         cudaFree(d_forced);
@@ -292,6 +295,40 @@ struct Engine {
         return cudaLaunchKernel(L.fn, dim3((unsigned)L.grid), dim3((unsigned)L.block), kargs, 0, stream);
     }
 
+    // Whether step k runs in a small-step run (k_small_run) when it is a single-step pass.
+    bool small_step(int k) const { return args[(size_t)k].nk <= SMALL_NK; }
+
+    // Steps k0 .. k1-1 as one k_small_run launch; norm: each step's norm pass runs before its write pass.
+    cudaError_t launch_small_run(int k0, int k1, int driver, bool norm, bool use_forced, bool use_unif) {
+        Launch L;
+        Ctx c = ctx(driver, plan.ns, L, use_forced, use_unif);
+        const StepArgs *sa = d_args;
+        int a0 = k0, a1 = k1, nm = norm ? 1 : 0;
+        void *memp = mem;
+        void *kargs[] = {&sa, &a0, &a1, &nm, &memp, &c};
+        void *fn = prec == 128 ? (void *)k_small_run<double2> : (void *)k_small_run<float2>;
+        return cudaLaunchKernel(fn, dim3(1), dim3(SMALL_THREADS), kargs, 0, stream);
+    }
+
+    // Length of the run of consecutive single small-step passes that starts at ops[i] (0 or 1: no run).
+    size_t small_run_len(const std::vector<Op> &ops, size_t i) const {
+        size_t j = i;
+        while (j < ops.size() && !ops[j].group && small_step(ops[j].k0)) j++;
+        return j - i >= 2 ? j - i : 0;
+    }
+
+    // Launches of one item over a pass list (small-step runs count once), begin and finish included.
+    int64_t item_launches(const std::vector<Op> &ops, bool norm) const {
+        int64_t n = 2;
+        for (size_t i = 0; i < ops.size();) {
+            const size_t r = small_run_len(ops, i);
+            if (r) { n++; i += r; continue; }
+            n += 1 + ((norm && !ops[i].group) || ops[i].norm_first ? 1 : 0);
+            i++;
+        }
+        return n;
+    }
+
     cudaError_t launch_begin() {
         if (prec == 128) k_begin<double2><<<1, 1, 0, stream>>>((double2 *)mem, st);
         else k_begin<float2><<<1, 1, 0, stream>>>((float2 *)mem, st);
@@ -318,15 +355,30 @@ struct Engine {
         cudaError_t e = launch_begin();
         if (e != cudaSuccess) return e;
         if (driver == DRV_CHAIN1 && !chain_ops.empty()) {
-            for (const Op &op : chain_ops) {
-                e = launch_op(op, driver);
+            for (size_t i = 0; i < chain_ops.size();) {
+                if (const size_t r = small_run_len(chain_ops, i)) {
+                    e = launch_small_run(chain_ops[i].k0, chain_ops[i + r - 1].k0 + 1, driver, false, use_forced,
+                                         use_unif);
+                    if (e != cudaSuccess) return e;
+                    i += r;
+                    continue;
+                }
+                e = launch_op(chain_ops[i++], driver);
                 if (e != cudaSuccess) return e;
             }
             k_finish<<<1, 1, 0, stream>>>(st, d_logp, d_aux, driver, plan.ns);
             return cudaGetLastError();
         }
         if (driver == DRV_CHAIN && !sample_ops.empty()) {
-            for (const Op &op : sample_ops) {
+            for (size_t i = 0; i < sample_ops.size();) {
+                if (const size_t r = small_run_len(sample_ops, i)) {
+                    e = launch_small_run(sample_ops[i].k0, sample_ops[i + r - 1].k0 + 1, driver, true, use_forced,
+                                         use_unif);
+                    if (e != cudaSuccess) return e;
+                    i += r;
+                    continue;
+                }
+                const Op &op = sample_ops[i++];
                 if (!op.group || op.norm_first) {
                     e = launch_step(op.k0, false, driver, plan.ns, use_forced, use_unif);
                     if (e != cudaSuccess) return e;
@@ -341,8 +393,14 @@ struct Engine {
         int k0 = 0;
         if (driver == DRV_HYBRID && hyb_K > 0) {
             // forced prefix: 'chain' passes (fused where possible), then the run_steps state for the sampled steps
-            for (const Op &op : hyb_ops) {
-                e = launch_op(op, DRV_CHAIN1);
+            for (size_t i = 0; i < hyb_ops.size();) {
+                if (const size_t r = small_run_len(hyb_ops, i)) {
+                    e = launch_small_run(hyb_ops[i].k0, hyb_ops[i + r - 1].k0 + 1, DRV_CHAIN1, false, true, false);
+                    if (e != cudaSuccess) return e;
+                    i += r;
+                    continue;
+                }
+                e = launch_op(hyb_ops[i++], DRV_CHAIN1);
                 if (e != cudaSuccess) return e;
             }
             k_hybrid_switch<<<1, 1, 0, stream>>>(st, d_forced, d_bits, plan.ns, hyb_K);
@@ -350,6 +408,14 @@ struct Engine {
             k0 = hyb_K;
         }
         for (int k = k0; k < plan.ns; k++) {
+            int k1 = k;
+            while (k1 < plan.ns && small_step(k1)) k1++;
+            if (k1 - k >= 2) {
+                e = launch_small_run(k, k1, driver, driver != DRV_CHAIN1, use_forced, use_unif);
+                if (e != cudaSuccess) return e;
+                k = k1 - 1;
+                continue;
+            }
             if (driver != DRV_CHAIN1) {
                 e = launch_step(k, false, driver, plan.ns, use_forced, use_unif);
                 if (e != cudaSuccess) return e;
@@ -366,6 +432,11 @@ struct Engine {
         if (it != graphs.end()) { *out = it->second; return 0; }
         int driver = kind == 0 ? DRV_CHAIN1 : kind == 3 ? DRV_HYBRID : DRV_CHAIN;
         bool use_forced = kind != 2, use_unif = kind >= 2;
+        if (args_dirty) {   // the small-step runs read the step descriptors from the device
+            GSB_CK(cudaMemcpyAsync(d_args, args.data(), args.size() * sizeof(StepArgs), cudaMemcpyHostToDevice, stream));
+            GSB_CK(cudaStreamSynchronize(stream));
+            args_dirty = false;
+        }
         cudaGraph_t g = nullptr;
         GSB_CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
         cudaError_t e = enqueue_item(driver, use_forced, use_unif);
@@ -475,6 +546,7 @@ static void apply_coeffs(Engine &E) {
                     E.args[(size_t)k].Mi32[b][x] = c.Mi[b][x];
                 }
     }
+    E.args_dirty = true;   // every change of the descriptors (matrices, arithmetic) ends here
 }
 
 static int make_args(Engine &E) {
@@ -512,6 +584,8 @@ static int make_args(Engine &E) {
     }
     maxgrid = std::max(maxgrid, (size_t)E.sms * 8);
     GSB_CK(cudaMalloc(&E.partials, maxgrid * 8 * sizeof(double)));   // up to 6 sums per block (fused groups)
+    GSB_CK(cudaMalloc(&E.d_args, (size_t)std::max(1, p.ns) * sizeof(StepArgs)));
+    E.args_dirty = true;
     return 0;
 }
 
@@ -646,10 +720,18 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
             a.cp[b] = fact ? cf.cp[b] : 1;
         }
         for (int j = 0; j < g.nmem; j++) {
-            for (int t = 0; t < g.ntq; t++) a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
+            for (int t = 0; t < g.ntq; t++) {
+                a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
+                a.ioff[j][t] = ((uint32_t)g.in_idx[j][t] << L) | (s == 0 ? ga.z0lo[j][t] : 0u);
+            }
             for (int tau = 0; tau < g.m; tau++) a.out_idx[j][tau] = (unsigned char)g.out_idx[j][tau];
             a.mpar[j] = (unsigned char)g.mpar[j];
         }
+    }
+    {
+        const GroupPlan::Step &gd = cs[gp.ws - 1];
+        for (int j = 0; j < gd.nmem; j++)
+            for (int tau = 0; tau < gd.m; tau++) ga.ooff[j][tau] = gp.z_out[(size_t)gd.out_idx[j][tau]];
     }
     if (fold) {
         // mode 2 when every trailing member reads one growth output in all its offsets
@@ -1937,7 +2019,19 @@ int gsb_launches_per_item(const gsb_engine *e, int mode, int64_t *launches) {
     if (!e || !launches) return fail(GSB_E_USAGE, "null argument");
     const Engine *E = eng(e);
     const int64_t ns = E->plan.ns;
-    *launches = mode == 0 ? (int64_t)E->chain_ops.size() + 2 : 2 * ns + 2;
+    if (mode == 0 && !E->chain_ops.empty()) *launches = E->item_launches(E->chain_ops, false);
+    else if (mode == 1 && !E->sample_ops.empty()) *launches = E->item_launches(E->sample_ops, true);
+    else {   // one norm and one write pass per step ('chain' mode: write only), small-step runs counted once
+        int64_t n = 2;
+        for (int k = 0; k < ns;) {
+            int k1 = k;
+            while (k1 < ns && E->small_step(k1)) k1++;
+            if (k1 - k >= 2) { n++; k = k1; continue; }
+            n += mode == 0 ? 1 : 2;
+            k++;
+        }
+        *launches = n;
+    }
     return 0;
 }
 

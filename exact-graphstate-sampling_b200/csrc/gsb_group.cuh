@@ -28,6 +28,9 @@ struct GroupStepArgs {
     int piv[2];
     double br[2], bi[2], cp[2];
     unsigned char in_idx[16][4], out_idx[16][2], mpar[16];
+    // member j, offset t: position of its value in the stage buffer (index << L), XORed for the first step with the
+    // low bits of its stage-0 offset (z0lo); a class pair's value sits at ioff ^ pc (factored complex64 passes)
+    uint32_t ioff[16][4];
 };
 
 // first-bit source of a sampling pass (group_decide)
@@ -52,6 +55,9 @@ struct GroupArgs {
     // its offsets (group_trail_fold2_pk)
     int fold;
     unsigned char fsrc[16][4], ftau[16][4], fmem[16][4];
+    // last written step: member j, output tau -> its whole written-stage offset (blk_out ^ zdlo): the class pair of a
+    // tile at base TB and position pc is stored at TB ^ ooff ^ pc (factored complex64 passes)
+    uint64_t ooff[16][2];
     GroupStepArgs st[3];
 };
 
@@ -657,19 +663,17 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
     }
     for (int j = j0; j < nm; j += jstride) {
         const int mp = tpar ^ gs.mpar[j];
-        uint32_t zl[NTQ], ib[NTQ];
+        // the member's positions come precomputed (GroupStepArgs::ioff, GroupArgs::ooff): one word per offset and
+        // output instead of an index, a multiply, the stage-0 / written-stage low bits and a block-table lookup
+        uint32_t io[NTQ];
 #pragma unroll
-        for (int t = 0; t < NTQ; t++) {
-            ib[t] = (uint32_t)gs.in_idx[j][t] * NC;
-            zl[t] = FIRST ? ga.z0lo[j][t] : 0u;
-        }
-        uint32_t ol[2] = {0, 0}, oidx[2] = {0, 0};
-        E *ob[2] = {mem, mem};
+        for (int t = 0; t < NTQ; t++) io[t] = gs.ioff[j][t];
+        uint32_t oidx[2] = {0, 0};
+        uint64_t oo[2] = {0, 0};
 #pragma unroll
         for (int tau = 0; tau < 2; tau++) {
-            oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
-            ol[tau] = LAST ? ga.zdlo[j][tau] : 0u;
-            if (LAST) ob[tau] = mem + (TB ^ ga.blk_out[gs.out_idx[j][tau]]);
+            if (LAST) oo[tau] = TB ^ ga.ooff[j][tau];
+            else oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
         }
         for (uint32_t g = g0; g < NG; g += gstride) {
             const uint32_t pc = (uint32_t)P * g;
@@ -682,11 +686,11 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
                 T vr[P], vi[P];
                 if (FIRST) {
                     if constexpr (P == 2 && std::is_same<T, float>::value)
-                        ld_pair16(reinterpret_cast<const float2 *>(smem + in) + ib[t], pc ^ zl[t], vr, vi);
+                        ld_pair16(reinterpret_cast<const float2 *>(smem + in), io[t] ^ pc, vr, vi);
                     else
-                        ld_perm<P>(reinterpret_cast<const E *>(smem + in) + ib[t], pc ^ zl[t], vr, vi);
+                        ld_perm<P>(reinterpret_cast<const E *>(smem + in), io[t] ^ pc, vr, vi);
                 } else {
-                    lds_cls<P>(reinterpret_cast<const V *>(smem + in) + (ib[t] + pc), vr, vi);
+                    lds_cls<P>(reinterpret_cast<const V *>(smem + in) + (io[t] ^ pc), vr, vi);
                 }
                 const int op = S::pout(t), oq = S::qout(t);
                 const bool p_first = S::first_p(op) == t, q_first = S::first_q(oq) == t;
@@ -732,10 +736,11 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
                     nsum = fmaT(im, im, nsum);
                 }
                 if (LAST) {
+                    const uint64_t q = oo[tau] ^ pc;
                     if constexpr (P == 2 && std::is_same<T, float>::value)
-                        st_pair16(reinterpret_cast<float2 *>(ob[tau]), pc ^ ol[tau], orr, oii);
+                        st_pair16(reinterpret_cast<float2 *>(mem) + (q & ~(uint64_t)1), (uint32_t)q & 1u, orr, oii);
                     else
-                        st_perm<P>(ob[tau], pc ^ ol[tau], orr, oii);
+                        st_perm<P>(mem + (q & ~(uint64_t)(P - 1)), (uint32_t)q & (uint32_t)(P - 1), orr, oii);
                 }
                 if (STS) sts_cls<P>(reinterpret_cast<V *>(smem + out) + (oidx[tau] + pc), orr, oii);
             }
@@ -790,19 +795,16 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
     f32x2 NS = 0ull;
     for (int j = j0; j < nm; j += jstride) {
         const int mp = tpar ^ gs.mpar[j];
-        uint32_t zl[NTQ], ib[NTQ];
+        // precomputed member positions, as in group_cosets_f
+        uint32_t io[NTQ];
 #pragma unroll
-        for (int t = 0; t < NTQ; t++) {
-            ib[t] = (uint32_t)gs.in_idx[j][t] * NC;
-            zl[t] = FIRST ? ga.z0lo[j][t] : 0u;
-        }
-        uint32_t ol[2] = {0, 0}, oidx[2] = {0, 0};
-        float2 *ob[2] = {mem, mem};
+        for (int t = 0; t < NTQ; t++) io[t] = gs.ioff[j][t];
+        uint32_t oidx[2] = {0, 0};
+        uint64_t oo[2] = {0, 0};
 #pragma unroll
         for (int tau = 0; tau < 2; tau++) {
-            oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
-            ol[tau] = LAST ? ga.zdlo[j][tau] : 0u;
-            if (LAST) ob[tau] = mem + (TB ^ ga.blk_out[gs.out_idx[j][tau]]);
+            if (STS) oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
+            if (LAST) oo[tau] = TB ^ ga.ooff[j][tau];
         }
         for (uint32_t g = g0; g < NG; g += gstride) {
             const uint32_t pc = 2u * g;
@@ -813,11 +815,11 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
                 f32x2 VR, VI;
                 if (FIRST) {
                     float r2[2], i2[2];
-                    ld_pair16(reinterpret_cast<const float2 *>(smem + in) + ib[t], pc ^ zl[t], r2, i2);
+                    ld_pair16(reinterpret_cast<const float2 *>(smem + in), io[t] ^ pc, r2, i2);
                     VR = f2_pack(r2[0], r2[1]);
                     VI = f2_pack(i2[0], i2[1]);
                 } else {
-                    const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (ib[t] + pc));
+                    const float4 v = *reinterpret_cast<const float4 *>(reinterpret_cast<const float2 *>(smem + in) + (io[t] ^ pc));
                     VR = f2_pack(v.x, v.y);
                     VI = f2_pack(v.z, v.w);
                 }
@@ -859,7 +861,8 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
                     f2_unpack(IM, i0, i1);
                     if (LAST) {
                         const float rr2[2] = {r0, r1}, ii2[2] = {i0, i1};
-                        st_pair16(ob[tau], pc ^ ol[tau], rr2, ii2);
+                        const uint64_t q = oo[tau] ^ pc;
+                        st_pair16(mem + (q & ~(uint64_t)1), (uint32_t)q & 1u, rr2, ii2);
                     }
                     if (STS)
                         *reinterpret_cast<float4 *>(reinterpret_cast<float2 *>(smem + out) + (oidx[tau] + pc)) =

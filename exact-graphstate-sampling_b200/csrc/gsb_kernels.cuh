@@ -315,6 +315,146 @@ __global__ void __launch_bounds__(256) k_step(const StepArgs s, E *__restrict__ 
 }
 
 // ---------------------------------------------------------------------------------------------------------------
+// A run of consecutive small steps (at most 2^SMALL_NK cosets each) in one launch of one CTA.  One k_step launch
+// per small step costs several microseconds of launch gap and dependent global round trips (state, partials,
+// counter) for a few kilobytes of table; the two ends of a string or sample are two dozen such steps.  Here the
+// CTA walks the steps itself: per step, the same coset arithmetic as k_step (FP64, in place on the arena; the
+// block's threads own disjoint cosets, and a block barrier separates the steps), the norm pass first when `norm` is
+// set (sampling and hybrid drivers; skipped for a forced hybrid step), a block-tree reduction in a fixed order, and
+// the same scalar epilogues run by thread 0.  Step descriptors come from the device copy of the engine's StepArgs.
+constexpr int SMALL_NK = 11;          // steps of up to 2^11 cosets join a run
+constexpr int SMALL_THREADS = 512;    // 4 cosets per thread at most
+constexpr int SMALL_U = (1 << SMALL_NK) / SMALL_THREADS;
+
+template <typename E>
+__global__ void __launch_bounds__(SMALL_THREADS) k_small_run(const StepArgs *__restrict__ sa, int k0, int k1, int norm,
+                                                             E *__restrict__ mem, const Ctx cx) {
+    __shared__ StepArgs s;
+    __shared__ double red[2][SMALL_THREADS / 32];
+    __shared__ int sh_skip, sh_bv;
+    __shared__ double sh_sc;
+    DevState *st = cx.st;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const size_t row = (size_t)st->item * (size_t)cx.ns;
+    for (int k = k0; k < k1; k++) {
+        __syncthreads();   // the previous step's readers of s and sh_* are done
+        {
+            const uint64_t *src = reinterpret_cast<const uint64_t *>(sa + k);
+            uint64_t *dst = reinterpret_cast<uint64_t *>(&s);
+            for (int i = tid; i < (int)(sizeof(StepArgs) / 8); i += SMALL_THREADS) dst[i] = src[i];
+        }
+        for (int ph = norm ? 0 : 1; ph < 2; ph++) {
+            const bool write = ph == 1;
+            if (ph == 1 && norm) __syncthreads();   // the norm phase's readers of sh_* are done
+            if (tid == 0) {
+                int skip = *(volatile int *)&st->dead;
+                int bv = 0;
+                double sc = 1.0;
+                if (!skip) {
+                    if (write) {
+                        if (cx.driver == DRV_HYBRID) {
+                            const int f = cx.forced[row + k];
+                            bv = f >= 0 ? f : st->bv;
+                            sc = 1.0 / sqrt(st->prev);
+                        } else if (cx.driver == DRV_CHAIN1) {
+                            bv = cx.forced[row + k];
+                            sc = st->sc;
+                        } else {
+                            bv = st->bv;
+                            sc = st->sc;
+                        }
+                    } else if (cx.driver == DRV_HYBRID && cx.forced[row + k] >= 0) {
+                        skip = 2;   // forced hybrid step: no norm pass
+                    }
+                }
+                sh_skip = skip;
+                sh_bv = bv;
+                sh_sc = sc;
+            }
+            __syncthreads();
+            if (sh_skip == 1) return;      // a zero-probability branch was taken: nothing more to do
+            if (sh_skip == 2) continue;
+            const int bv = sh_bv;
+            const double sc = sh_sc;
+            const uint64_t N = 1ULL << s.nk;
+            const int ntq = s.ntq, mout = s.m;
+            const double m0r = bv ? s.Mr[1][0] : s.Mr[0][0], m0i = bv ? s.Mi[1][0] : s.Mi[0][0];
+            const double m1r = bv ? s.Mr[1][1] : s.Mr[0][1], m1i = bv ? s.Mi[1][1] : s.Mi[0][1];
+            double a0 = 0, a1 = 0;
+            double vr[SMALL_U][4], vi[SMALL_U][4];
+            uint64_t base[SMALL_U];
+#pragma unroll
+            for (int u = 0; u < SMALL_U; u++) {
+                const uint64_t c = (uint64_t)tid + (uint64_t)u * SMALL_THREADS;
+                base[u] = c < N ? xor_cols(s.tk, c) : 0;
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+                    if (c < N && i < ntq) load_entry(mem + (base[u] ^ s.tq[i]), vr[u][i], vi[u][i]);
+            }
+#pragma unroll
+            for (int u = 0; u < SMALL_U; u++) {
+                const uint64_t c = (uint64_t)tid + (uint64_t)u * SMALL_THREADS;
+                if (c >= N) continue;
+                const int pc = __popcll(c & s.rhoc) & 1;
+                double s00r = 0, s00i = 0, s01r = 0, s01i = 0, s10r = 0, s10i = 0, s11r = 0, s11i = 0;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (i >= ntq) break;
+                    const double xr = vr[u][i], xi = vi[u][i];
+                    if (mout == 1 || s.tau0[i] == 0) { s00r += xr; s00i += xi; }
+                    else { s01r += xr; s01i += xi; }
+                    const bool neg = (pc ^ s.par[i]) != 0;
+                    const double yr = neg ? -xr : xr, yi = neg ? -xi : xi;
+                    if (mout == 1 || s.tau1[i] == 0) { s10r += yr; s10i += yi; }
+                    else { s11r += yr; s11i += yi; }
+                }
+                if (write) {
+                    double o0r = m0r * s00r - m0i * s00i + m1r * s10r - m1i * s10i;
+                    double o0i = m0r * s00i + m0i * s00r + m1r * s10i + m1i * s10r;
+                    o0r *= sc;
+                    o0i *= sc;
+                    store_entry(mem + base[u], o0r, o0i);
+                    a0 += o0r * o0r + o0i * o0i;
+                    if (mout == 2) {
+                        double o1r = m0r * s01r - m0i * s01i + m1r * s11r - m1i * s11i;
+                        double o1i = m0r * s01i + m0i * s01r + m1r * s11i + m1i * s11r;
+                        o1r *= sc;
+                        o1i *= sc;
+                        store_entry(mem + (base[u] ^ s.g), o1r, o1i);
+                        a0 += o1r * o1r + o1i * o1i;
+                    }
+                } else {
+#pragma unroll
+                    for (int bb = 0; bb < 2; bb++) {
+                        const double p0r = s.Mr[bb][0], p0i = s.Mi[bb][0], p1r = s.Mr[bb][1], p1i = s.Mi[bb][1];
+                        const double o0r = p0r * s00r - p0i * s00i + p1r * s10r - p1i * s10i;
+                        const double o0i = p0r * s00i + p0i * s00r + p1r * s10i + p1i * s10r;
+                        double nn = o0r * o0r + o0i * o0i;
+                        if (mout == 2) {
+                            const double o1r = p0r * s01r - p0i * s01i + p1r * s11r - p1i * s11i;
+                            const double o1i = p0r * s01i + p0i * s01r + p1r * s11i + p1i * s11r;
+                            nn += o1r * o1r + o1i * o1i;
+                        }
+                        if (bb == 0) a0 += nn;
+                        else a1 += nn;
+                    }
+                }
+            }
+            a0 = warp_sum(a0);
+            a1 = warp_sum(a1);
+            if (lane == 0) { red[0][warp] = a0; red[1][warp] = a1; }
+            __syncthreads();   // the partial sums, and every store of this pass, are visible to the block
+            if (tid == 0) {
+                double t0 = 0, t1 = 0;
+                for (int w = 0; w < SMALL_THREADS / 32; w++) { t0 += red[0][w]; t1 += red[1][w]; }
+                if (write) write_epilogue(cx, k, bv, t0);
+                else norm_epilogue(cx, k, t0, t1);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------------------------
 // Wide-step kernels.  Steps with at least 2^11 cosets run one of these instead of k_step; both
 //   * walk their block's range of chunks in Gray-code order, so consecutive chunks differ in one coset bit and the
 //     chunk's base address is updated with one XOR (chunk i covers cosets gray(i) * 2^chunk_log2 + [0, 2^chunk_log2));
