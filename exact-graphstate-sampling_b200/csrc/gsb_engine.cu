@@ -724,7 +724,10 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
                 a.in_idx[j][t] = (unsigned char)g.in_idx[j][t];
                 a.ioff[j][t] = ((uint32_t)g.in_idx[j][t] << L) | (s == 0 ? ga.z0lo[j][t] : 0u);
             }
-            for (int tau = 0; tau < g.m; tau++) a.out_idx[j][tau] = (unsigned char)g.out_idx[j][tau];
+            for (int tau = 0; tau < g.m; tau++) {
+                a.out_idx[j][tau] = (unsigned char)g.out_idx[j][tau];
+                a.soff[j][tau] = (uint32_t)g.out_idx[j][tau] << L;
+            }
             a.mpar[j] = (unsigned char)g.mpar[j];
         }
     }

@@ -31,6 +31,7 @@ struct GroupStepArgs {
     // member j, offset t: position of its value in the stage buffer (index << L), XORed for the first step with the
     // low bits of its stage-0 offset (z0lo); a class pair's value sits at ioff ^ pc (factored complex64 passes)
     uint32_t ioff[16][4];
+    uint32_t soff[16][2];   // member j, output tau: position of its stage-(s+1) value (index << L)
 };
 
 // first-bit source of a sampling pass (group_decide)
@@ -620,14 +621,13 @@ struct FShape {
     }
 };
 
-template <typename E, typename T, int P, int NTQ, int H, int PIV, bool SC, bool FIRST, bool LAST, bool STS>
+template <typename E, typename T, int P, int NTQ, int H, int PIV, bool SC, bool FIRST, bool LAST, bool STS, int NM = 0>
 __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupStepArgs &gs, E *__restrict__ mem,
                                                const uint64_t TB, const int L, const uint32_t in, const uint32_t out,
                                                const T sc, const T br, const T bi, T &nsum) {
     typedef typename CplxOf<T>::type V;
     typedef FShape<NTQ, H, PIV> S;
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t NC = 1u << L;
     const int LG = L - (P == 2 ? 1 : 0);
     const uint32_t NG = 1u << LG;
     const int tpar = __popcll(TB & gs.lambda) & 1;
@@ -661,25 +661,13 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
         rel[t] = PIV == 0 ? sg[t] * sg[f < 0 ? 0 : f] : (T)1;
         pcf[t] = PIV == 0 ? sc : sc * sg[t];
     }
-    for (int j = j0; j < nm; j += jstride) {
-        const int mp = tpar ^ gs.mpar[j];
-        // the member's positions come precomputed (GroupStepArgs::ioff, GroupArgs::ooff): one word per offset and
-        // output instead of an index, a multiply, the stage-0 / written-stage low bits and a block-table lookup
-        uint32_t io[NTQ];
-#pragma unroll
-        for (int t = 0; t < NTQ; t++) io[t] = gs.ioff[j][t];
-        uint32_t oidx[2] = {0, 0};
-        uint64_t oo[2] = {0, 0};
-#pragma unroll
-        for (int tau = 0; tau < 2; tau++) {
-            if (LAST) oo[tau] = TB ^ ga.ooff[j][tau];
-            else oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
-        }
-        for (uint32_t g = g0; g < NG; g += gstride) {
-            const uint32_t pc = (uint32_t)P * g;
+    // one member's class pair at position pc: mpp = the class sign parity of the pair's even class before the
+    // member's own parity bit is applied (mp ^ parity(pc & lambda))
+    auto member = [&](const uint32_t (&io)[NTQ], const uint32_t (&oidx)[2], const uint64_t (&oo)[2], const uint32_t pc,
+                      const int mpp) {
             bool neg[P];
 #pragma unroll
-            for (int c = 0; c < P; c++) neg[c] = ((mp ^ __popc(pc & lam) ^ __popc((uint32_t)c & lam)) & 1) != 0;
+            for (int c = 0; c < P; c++) neg[c] = ((mpp ^ __popc((uint32_t)c & lam)) & 1) != 0;
             T pr[P][2], pi[P][2], qr[P][2], qi[P][2];
 #pragma unroll
             for (int t = 0; t < NTQ; t++) {
@@ -744,7 +732,49 @@ __device__ __forceinline__ void group_cosets_f(const GroupArgs &ga, const GroupS
                 }
                 if (STS) sts_cls<P>(reinterpret_cast<V *>(smem + out) + (oidx[tau] + pc), orr, oii);
             }
+    };
+    if constexpr (NM > 0) {
+        // compile-time member count (warp-specialised passes, tiles of 2^9 classes or more, so NG >= GROUP_NCT and
+        // every thread runs every member of its class pairs): members unrolled inside the class-pair loop, their
+        // descriptors constant operands, the pair's sign parity formed once
+        for (uint32_t g = threadIdx.x; g < NG; g += GROUP_NCT) {
+            const uint32_t pc = (uint32_t)P * g;
+            const int pp = tpar ^ __popc(pc & lam);
+#pragma unroll
+            for (int j = 0; j < NM; j++) {
+                uint32_t io[NTQ];
+#pragma unroll
+                for (int t = 0; t < NTQ; t++) io[t] = gs.ioff[j][t];
+                uint32_t oidx[2] = {0, 0};
+                uint64_t oo[2] = {0, 0};
+#pragma unroll
+                for (int tau = 0; tau < 2; tau++) {
+                    if (LAST) oo[tau] = TB ^ ga.ooff[j][tau];
+                    else oidx[tau] = gs.soff[j][tau];
+                }
+                member(io, oidx, oo, pc, pp ^ gs.mpar[j]);
+            }
         }
+    } else {
+    for (int j = j0; j < nm; j += jstride) {   // runtime member count
+        const int mp = tpar ^ gs.mpar[j];
+        // the member's positions come precomputed (GroupStepArgs::ioff, GroupArgs::ooff): one word per offset and
+        // output instead of an index, a multiply, the stage-0 / written-stage low bits and a block-table lookup
+        uint32_t io[NTQ];
+#pragma unroll
+        for (int t = 0; t < NTQ; t++) io[t] = gs.ioff[j][t];
+        uint32_t oidx[2] = {0, 0};
+        uint64_t oo[2] = {0, 0};
+#pragma unroll
+        for (int tau = 0; tau < 2; tau++) {
+            if (LAST) oo[tau] = TB ^ ga.ooff[j][tau];
+            else oidx[tau] = gs.soff[j][tau];
+        }
+        for (uint32_t g = g0; g < NG; g += gstride) {
+            const uint32_t pc = (uint32_t)P * g;
+            member(io, oidx, oo, pc, mp ^ __popc(pc & lam));
+        }
+    }
     }
 }
 
@@ -756,7 +786,6 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
                                                  const float sc, const float br, const float bi, float &nsum) {
     typedef FShape<NTQ, H, PIV> S;
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t NC = 1u << L;
     const int LG = L - 1;
     const uint32_t NG = 1u << LG;
     const int tpar = __popcll(TB & gs.lambda) & 1;
@@ -803,7 +832,7 @@ __device__ __forceinline__ void group_cosets_pkf(const GroupArgs &ga, const Grou
         uint64_t oo[2] = {0, 0};
 #pragma unroll
         for (int tau = 0; tau < 2; tau++) {
-            if (STS) oidx[tau] = (uint32_t)gs.out_idx[j][tau] * NC;
+            if (STS) oidx[tau] = gs.soff[j][tau];
             if (LAST) oo[tau] = TB ^ ga.ooff[j][tau];
         }
         for (uint32_t g = g0; g < NG; g += gstride) {
@@ -1387,7 +1416,7 @@ __device__ __forceinline__ void group_trail64(const GroupArgs &ga, const GroupSt
 
 // A written step of a complex64 pass: the factored form when the step has a compile-time shape and a pivot (piv >= 0,
 // GroupStepArgs::piv), else the general form with the scaled M row (w_r, w_i).
-template <typename T, bool SC, bool FIRST, bool LAST, bool STS, bool PK>
+template <typename T, bool SC, bool FIRST, bool LAST, bool STS, bool PK, bool UM = false>
 __device__ __forceinline__ void group_written64(const GroupArgs &ga, const GroupStepArgs &gs, float2 *__restrict__ mem,
                                                 const uint64_t TB, const int L, const uint32_t in, const uint32_t out,
                                                 const int piv, const T sc, const T br, const T bi,
@@ -1412,7 +1441,22 @@ __device__ __forceinline__ void group_written64(const GroupArgs &ga, const Group
             }
 #undef GSB_GF
         } else {
-#define GSB_GF(NTQ_, H_, P_) group_cosets_f<float2, T, 2, NTQ_, H_, P_, SC, FIRST, LAST, STS>(ga, gs, mem, TB, L, in, out, sc, br, bi, nsum)
+// UM (warp-specialised passes): the common member counts 1, 2 and 4 at compile time
+#define GSB_GFN(NTQ_, H_, P_, NM_) \
+    group_cosets_f<float2, T, 2, NTQ_, H_, P_, SC, FIRST, LAST, STS, NM_>(ga, gs, mem, TB, L, in, out, sc, br, bi, nsum)
+#define GSB_GF(NTQ_, H_, P_)                                             \
+    do {                                                                 \
+        if constexpr (UM) {                                              \
+            switch (gs.nmem) {                                           \
+                case 1: GSB_GFN(NTQ_, H_, P_, 1); break;                 \
+                case 2: GSB_GFN(NTQ_, H_, P_, 2); break;                 \
+                case 4: GSB_GFN(NTQ_, H_, P_, 4); break;                 \
+                default: GSB_GFN(NTQ_, H_, P_, 0); break;                \
+            }                                                            \
+        } else {                                                         \
+            GSB_GFN(NTQ_, H_, P_, 0);                                    \
+        }                                                                \
+    } while (0)
             switch (gs.kind * 2 + piv) {
                 case GK_1_0 * 2: GSB_GF(1, 0, 0); break;
                 case GK_1_0 * 2 + 1: GSB_GF(1, 0, 1); break;
@@ -1428,6 +1472,7 @@ __device__ __forceinline__ void group_written64(const GroupArgs &ga, const Group
                 default: GSB_GF(4, 2, 1); break;
             }
 #undef GSB_GF
+#undef GSB_GFN
         }
         return;
     }
@@ -1748,10 +1793,10 @@ __global__ void __launch_bounds__(WS ? GROUP_NCT + 32 : GROUP_NCT, MINB)
         if constexpr (FACT) {
             float2 *m64 = reinterpret_cast<float2 *>(mem);
             if (D == 1)
-                group_written64<T, true, true, true, TR == 1, PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
+                group_written64<T, true, true, true, TR == 1, PK, WS && !PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
                                                                  fsc[0], fbr[0], fbi[0], w[0], wj[0], ns[0][0][0]);
             else
-                group_written64<T, true, true, false, true, PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
+                group_written64<T, true, true, false, true, PK, WS && !PK>(ga, ga.st[0], m64, TB, L, tin[0], sm.mid[1], fpiv[0],
                                                                fsc[0], fbr[0], fbi[0], w[0], wj[0], ns[0][0][0]);
         } else if (D == 1) {
             group_cosets_any<E, T, true, true, TR == 1, 1, 1, PK>(ga, ga.st[0], mem, TB, L, tin, m1o, w[0], wj[0], ns[0]);
@@ -1774,22 +1819,22 @@ __global__ void __launch_bounds__(WS ? GROUP_NCT + 32 : GROUP_NCT, MINB)
         if constexpr (FACT) {
             float2 *m64 = reinterpret_cast<float2 *>(mem);
             if (FOLD && ga.fold) {   // the written stage is not kept: the trailing step folds it
-                group_written64<T, false, false, true, false, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], 0u,
+                group_written64<T, false, false, true, false, PK, WS && !PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], 0u,
                                                                  fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
                                                                  fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
                                                                  w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
             } else if (D == 2) {
-                group_written64<T, false, false, true, TR == 1, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
+                group_written64<T, false, false, true, TR == 1, PK, WS && !PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
                                                                    fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
                                                                    fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
                                                                    w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
             } else if (D == 3) {
-                group_written64<T, false, false, false, true, PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
+                group_written64<T, false, false, false, true, PK, WS && !PK>(ga, ga.st[1], m64, TB, L, sm.mid[1], sm.mid[2],
                                                                  fpiv[D > 1 ? 1 : 0], fsc[D > 1 ? 1 : 0],
                                                                  fbr[D > 1 ? 1 : 0], fbi[D > 1 ? 1 : 0],
                                                                  w[D > 1 ? 1 : 0], wj[D > 1 ? 1 : 0], ns[D > 1 ? 1 : 0][0][0]);
                 if constexpr (!WS) __syncthreads();
-                group_written64<T, false, false, true, false, PK>(ga, ga.st[2], m64, TB, L, sm.mid[2], 0u,
+                group_written64<T, false, false, true, false, PK, WS && !PK>(ga, ga.st[2], m64, TB, L, sm.mid[2], 0u,
                                                                  fpiv[D > 2 ? 2 : 0], fsc[D > 2 ? 2 : 0],
                                                                  fbr[D > 2 ? 2 : 0], fbi[D > 2 ? 2 : 0],
                                                                  w[D > 2 ? 2 : 0], wj[D > 2 ? 2 : 0], ns[D > 2 ? 2 : 0][0][0]);
