@@ -20,8 +20,12 @@ CLI128 = os.path.join(HERE, "gsb2_c128")
 
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall"]
-LIB_SOURCES = ["gsb_engine.cu", "gsb_dp.cu", "gsb_grad.cu", "gsb_batch.cu", "gsb_probe.cu", "gsb_plan.cpp", "gsb_order.cpp", "gsb_fuse.cpp"]
-LIB_DEPS = LIB_SOURCES + ["gsb_kernels.cuh", "gsb_group.cuh", "gsb_step.h", "gsb_plan.h", "gsb_common.h", "gsb_fuse.h"]
+# the complex64 FP32 fused passes sit in translation units of their own (gsb_group_*.cu): the largest objects, compiled
+# in parallel with the rest
+LIB_SOURCES = ["gsb_engine.cu", "gsb_group_ws.cu", "gsb_group_wst.cu", "gsb_group_f32.cu", "gsb_group3.cu",
+               "gsb_dp.cu", "gsb_grad.cu", "gsb_batch.cu", "gsb_probe.cu", "gsb_plan.cpp", "gsb_order.cpp", "gsb_fuse.cpp"]
+LIB_DEPS = LIB_SOURCES + ["gsb_kernels.cuh", "gsb_group.cuh", "gsb_step.h", "gsb_plan.h", "gsb_common.h", "gsb_fuse.h",
+                          "gsb_pick.h"]
 
 
 def _nvcc():

@@ -25,6 +25,7 @@
 #include "gsb_fuse.h"
 #include "gsb_group.cuh"
 #include "gsb_kernels.cuh"
+#include "gsb_pick.h"
 #include "gsb_plan.h"
 
 namespace gsb {
@@ -109,16 +110,6 @@ template <typename E, typename T>
 static void *pick_group(int d, int tr) {
     if (tr) return d == 2 ? (void *)k_group<E, T, 2, 1> : (void *)k_group<E, T, 1, 1>;
     return d == 3 ? (void *)k_group<E, T, 3, 0> : (void *)k_group<E, T, 2, 0>;
-}
-// the warp-specialised instantiations (complex64, FP32 arithmetic, tiles of 2^9 classes or more)
-static void *pick_group_ws(int d, int tr) {
-    if (tr) return d == 2 ? (void *)k_group<float2, float, 2, 1, 2, true> : (void *)k_group<float2, float, 1, 1, 2, true>;
-    return d == 3 ? (void *)k_group<float2, float, 3, 0, 2, true> : (void *)k_group<float2, float, 2, 0, 2, true>;
-}
-// the three-CTAs-per-SM instantiations (complex64, FP32 arithmetic)
-static void *pick_group3(int d, int tr) {
-    if (tr) return d == 2 ? (void *)k_group<float2, float, 2, 1, 3> : (void *)k_group<float2, float, 1, 1, 3>;
-    return d == 3 ? (void *)k_group<float2, float, 3, 0, 3> : (void *)k_group<float2, float, 2, 0, 3>;
 }
 
 // One pass of an item: a single step (group == false: norm pass + write pass when sampling) or a fused group that
@@ -766,7 +757,8 @@ static bool fill_group(Engine &E, const GroupPlan &gp, Op &op, int lcap = GROUP_
     if (E.prec == 128) op.fn = pick_group<double2, double>(op.d, op.tr);
     else if (E.arith == 64) op.fn = pick_group<float2, double>(op.d, op.tr);
     else if (minb == 3) op.fn = pick_group3(op.d, op.tr);
-    else op.fn = ws ? pick_group_ws(op.d, op.tr) : pick_group<float2, float>(op.d, op.tr);
+    else if (ws) op.fn = pick_group_ws(op.d, op.tr);
+    else op.fn = pick_group_f32(op.d, op.tr);
     if (cudaFuncSetAttribute(op.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)GROUP_SMEM_BUDGET) != cudaSuccess)
         return false;
     int nb = 0;

@@ -748,7 +748,7 @@ __global__ void k_begin(E *mem, DevState *st) {
 }
 
 // End of a string / sample: final log2 Pr, next item.
-__global__ void k_finish(DevState *st, double *logp_out, double *aux_out, int driver, int ns) {
+static __global__ void k_finish(DevState *st, double *logp_out, double *aux_out, int driver, int ns) {
     const int it = st->item;
     double lp;
     if (driver == DRV_CHAIN1) lp = st->dead ? -INFINITY : log2(st->prev) + 2.0 * st->lsc - ns;
@@ -758,12 +758,12 @@ __global__ void k_finish(DevState *st, double *logp_out, double *aux_out, int dr
     st->item = it + 1;
 }
 
-__global__ void k_set_item(DevState *st, int item) { st->item = item; }
+static __global__ void k_set_item(DevState *st, int item) { st->item = item; }
 
 // Hybrid item whose first K steps are forced and ran as 'chain' passes (DRV_CHAIN1): from here on the run_steps
 // conventions (gsamp2.cpp:77-98).  The stored table is the true one times 2^-lsc, which is run_steps' logscale;
 // log2 Pr of the prefix is log2 |table|^2 + 2 lsc - K.  The forced bits of the prefix go to the output row.
-__global__ void k_hybrid_switch(DevState *st, const int8_t *forced, int8_t *bits_out, int ns, int K) {
+static __global__ void k_hybrid_switch(DevState *st, const int8_t *forced, int8_t *bits_out, int ns, int K) {
     const size_t row = (size_t)st->item * (size_t)ns;
     for (int k = 0; k < K; k++) bits_out[row + k] = forced[row + k];
     if (st->dead) {   // a zero-probability prefix: the chain epilogue zeroed every conditional from there on
