@@ -114,6 +114,9 @@ static void *pick_group(int d, int tr) {
 
 // One pass of an item: a single step (group == false: norm pass + write pass when sampling) or a fused group that
 // writes d steps and, with tr = 1, evaluates the next step's branch norms (sampling only).
+// A fused pass's kernel parameters (GroupArgs, the arena pointer, Ctx) stay within the 4 KB of a classic launch.
+static_assert(sizeof(GroupArgs) + sizeof(void *) + sizeof(Ctx) <= 4096, "fused-pass parameters exceed 4 KB");
+
 struct Op {
     int k0 = 0, d = 1, tr = 0, lcap = 0;   // lcap: the tile-size cap the pass was built with (fused passes)
     int minb = 2;                          // CTAs per SM the fused kernel is built for (2, or 3: pick_group3)
